@@ -1,0 +1,312 @@
+// The C-ABI entry points (include/ccoil_gpu.h): argument checks, device
+// buffers, host<->device staging and kernel dispatch.  Nothing here exits the
+// process: every failure becomes a status code plus a thread-local message.
+#include "ccoil_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+
+namespace ccoil
+{
+namespace
+{
+thread_local std::string t_error;
+
+// Grow-only device buffer owned by a plan.
+struct DeviceBuffer
+{
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t n);
+    void release()
+    {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+} // namespace
+
+void setError(const std::string &msg) { t_error = msg; }
+
+int fail(int status, const std::string &msg)
+{
+    t_error = msg;
+    return status;
+}
+
+int cudaFail(cudaError_t e, const char *what)
+{
+    if (e == cudaErrorMemoryAllocation)
+        return fail(CCOIL_ERR_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return fail(CCOIL_ERR_NO_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(CCOIL_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace
+{
+int DeviceBuffer::reserve(size_t n)
+{
+    if (n <= bytes)
+        return CCOIL_OK;
+    release();
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess)
+    {
+        ptr = nullptr;
+        return cudaFail(e, "cudaMalloc");
+    }
+    bytes = n;
+    return CCOIL_OK;
+}
+
+int autoLanes(long long npts)
+{
+    // enough threads to fill the 148 SMs several times over; below that, split
+    // the angular nodes of each point across lanes
+    const long long target = 148LL * 1024;
+    int lanes = 1;
+    while (lanes < 8 && npts * lanes < target)
+        lanes *= 2;
+    return lanes;
+}
+
+bool validLanes(int l) { return l == 1 || l == 2 || l == 4 || l == 8 || l == 16 || l == 32; }
+} // namespace
+} // namespace ccoil
+
+using namespace ccoil;
+
+struct ccoil_field_plan
+{
+    int field = 0;
+    int precision = 0;
+    int coil_count = 0;
+    SegmentSet set;
+    DeviceBuffer blob, segs, points, out;
+};
+
+extern "C" {
+
+int ccoil_abi_version(void) { return CCOIL_ABI_VERSION; }
+
+const char *ccoil_last_error_message(void) { return t_error.c_str(); }
+
+int ccoil_coil_init(double inner_radius, double thickness, double length, int num_turns, double current,
+                    double sine_frequency, const double position[3], double y_axis_angle, double z_axis_angle,
+                    double precision_factor, int gpu_increments, ccoil_coil_t *out)
+{
+    if (!out)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "out is null");
+    if (!(inner_radius > 0.0) || thickness < 0.0 || length < 0.0 || num_turns < 1 || gpu_increments < 0 ||
+        gpu_increments > kMaxOrder)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT,
+                    "coil needs inner_radius > 0, thickness >= 0, length >= 0, num_turns >= 1, "
+                    "gpu_increments in [0, 100]");
+    initCoil(inner_radius, thickness, length, num_turns, current, sine_frequency, position, y_axis_angle,
+             z_axis_angle, *out);
+    out->precision = coilPrecision(*out, precision_factor, gpu_increments);
+    return CCOIL_OK;
+}
+
+int ccoil_precision_arguments(const ccoil_coil_t *coil, double precision_factor, int gpu_increments,
+                              ccoil_precision_args_t *out)
+{
+    if (!coil || !out)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "null argument");
+    if (gpu_increments < 0 || gpu_increments > kMaxOrder)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "gpu_increments must be in [0, 100]");
+    *out = coilPrecision(*coil, precision_factor, gpu_increments);
+    return CCOIL_OK;
+}
+
+int ccoil_pair_arguments(const ccoil_coil_t *primary, const ccoil_coil_t *secondary, double precision_factor,
+                         int gpu_increments, int z_axis_case, int pure_gpu, ccoil_precision_args_t *primary_out,
+                         ccoil_precision_args_t *secondary_out)
+{
+    if (!primary || !secondary || !primary_out || !secondary_out)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "null argument");
+    if (gpu_increments < 0 || gpu_increments > kMaxOrder)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "gpu_increments must be in [0, 100]");
+    pairPrecision(*primary, *secondary, precision_factor, gpu_increments, z_axis_case != 0, pure_gpu != 0,
+                  *primary_out, *secondary_out);
+    return CCOIL_OK;
+}
+
+int ccoil_legendre(int order, double *nodes, double *weights)
+{
+    if (order < 1 || order > kMaxOrder || !nodes || !weights)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "order must be in [1, 100] and buffers non-null");
+    std::memcpy(nodes, legendreNodes(order), sizeof(double) * order);
+    std::memcpy(weights, legendreWeights(order), sizeof(double) * order);
+    return CCOIL_OK;
+}
+
+int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field, int precision,
+                            ccoil_field_plan_t **plan)
+{
+    if (!plan)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "plan is null");
+    *plan = nullptr;
+    if (coil_count < 0 || (coil_count > 0 && !coils))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "coil_count < 0 or coils null");
+    if (field < CCOIL_FIELD_A || field > CCOIL_FIELD_G)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "field must be A, B, E or G");
+    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "precision must be FP64 or FP32_COMPENSATED");
+    if (precision == CCOIL_PRECISION_FP32_COMPENSATED)
+        return fail(CCOIL_ERR_NOT_SUPPORTED, "FP32_COMPENSATED fields are not built in this library version");
+
+    ccoil_field_plan *p = new (std::nothrow) ccoil_field_plan();
+    if (!p)
+        return fail(CCOIL_ERR_OUT_OF_MEMORY, "host allocation failed");
+    p->field = field;
+    p->precision = precision;
+    p->coil_count = coil_count;
+    std::string err;
+    if (!buildFieldSegments(coils, coil_count, field, precision, p->set, err))
+    {
+        delete p;
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, err);
+    }
+    if (!p->set.segs.empty())
+    {
+        int rc = p->blob.reserve(p->set.blob.size());
+        if (rc == CCOIL_OK)
+            rc = p->segs.reserve(sizeof(SegmentDesc) * p->set.segs.size());
+        if (rc != CCOIL_OK)
+        {
+            ccoil_field_plan_destroy(p);
+            return rc;
+        }
+        cudaError_t e = cudaMemcpy(p->blob.ptr, p->set.blob.data(), p->set.blob.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(p->segs.ptr, p->set.segs.data(), sizeof(SegmentDesc) * p->set.segs.size(),
+                           cudaMemcpyHostToDevice);
+        if (e != cudaSuccess)
+        {
+            ccoil_field_plan_destroy(p);
+            return cudaFail(e, "cudaMemcpy");
+        }
+    }
+    *plan = p;
+    return CCOIL_OK;
+}
+
+int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, long long point_count, double *out,
+                             int memory, int lanes_per_point, void *stream)
+{
+    if (!plan)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "plan is null");
+    if (point_count < 0 || (point_count > 0 && (!points || !out)))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "point_count < 0 or null points/out");
+    if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
+    if (lanes_per_point != 0 && !validLanes(lanes_per_point))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "lanes_per_point must be 0, 1, 2, 4, 8, 16 or 32");
+    if (point_count == 0)
+        return CCOIL_OK;
+    // grid.x limit: 2^31-1 CTAs of 128/lanes points
+    if (point_count > (1LL << 36))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "point_count above 2^36");
+
+    const int width = plan->field == CCOIL_FIELD_G ? 9 : 3;
+    const size_t inBytes = sizeof(double) * 3 * (size_t)point_count;
+    const size_t outBytes = sizeof(double) * width * (size_t)point_count;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    const double *dPoints = points;
+    double *dOut = out;
+    if (memory == CCOIL_MEMORY_HOST)
+    {
+        int rc = plan->points.reserve(inBytes);
+        if (rc == CCOIL_OK)
+            rc = plan->out.reserve(outBytes);
+        if (rc != CCOIL_OK)
+            return rc;
+        cudaError_t e = cudaMemcpyAsync(plan->points.ptr, points, inBytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess)
+            return cudaFail(e, "host->device copy of points");
+        dPoints = static_cast<const double *>(plan->points.ptr);
+        dOut = static_cast<double *>(plan->out.ptr);
+    }
+
+    FieldLaunch L;
+    L.d_blob = static_cast<const unsigned char *>(plan->blob.ptr);
+    L.d_segs = static_cast<const SegmentDesc *>(plan->segs.ptr);
+    L.nseg = (int)plan->set.segs.size();
+    L.d_points = dPoints;
+    L.npts = point_count;
+    L.d_out = dOut;
+    L.field = plan->field;
+    L.precision = plan->precision;
+    L.lanes = lanes_per_point ? lanes_per_point : autoLanes(point_count);
+    int rc = launchFields(L, stream);
+    if (rc != CCOIL_OK)
+        return rc;
+
+    if (memory == CCOIL_MEMORY_HOST)
+    {
+        cudaError_t e = cudaMemcpyAsync(out, dOut, outBytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            return cudaFail(e, "field evaluation");
+        long long timeouts = 0;
+        rc = readTimeouts(timeouts);
+        if (rc != CCOIL_OK)
+            return rc;
+        static thread_local long long seen = 0;
+        if (timeouts > seen)
+        {
+            seen = timeouts;
+            return fail(CCOIL_ERR_TIMEOUT, "a staging wait in the field kernel timed out");
+        }
+    }
+    return CCOIL_OK;
+}
+
+int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
+{
+    if (!plan)
+        return CCOIL_OK;
+    plan->blob.release();
+    plan->segs.release();
+    plan->points.release();
+    plan->out.release();
+    delete plan;
+    return CCOIL_OK;
+}
+
+int ccoil_compute_fields(const ccoil_coil_t *coils, int coil_count, const double *points, long long point_count,
+                         int field, int precision, double *out, int memory, void *stream)
+{
+    ccoil_field_plan_t *plan = nullptr;
+    int rc = ccoil_field_plan_create(coils, coil_count, field, precision, &plan);
+    if (rc != CCOIL_OK)
+        return rc;
+    rc = ccoil_field_plan_execute(plan, points, point_count, out, memory, 0, stream);
+    if (memory == CCOIL_MEMORY_DEVICE && rc == CCOIL_OK)
+    {
+        // the plan's device tables must outlive the asynchronous kernel
+        cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess)
+            rc = cudaFail(e, "field evaluation");
+    }
+    ccoil_field_plan_destroy(plan);
+    return rc;
+}
+
+long long ccoil_timeout_count(void)
+{
+    long long v = 0;
+    if (readTimeouts(v) != CCOIL_OK)
+        return -1;
+    return v;
+}
+
+} // extern "C"

@@ -1,0 +1,112 @@
+// Internal declarations shared by the host code and the CUDA kernels.
+#ifndef CCOIL_INTERNAL_H
+#define CCOIL_INTERNAL_H
+
+#include "../../include/ccoil_gpu.h"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace ccoil
+{
+using Coil = ccoil_coil_t;
+using PrecisionArgs = ccoil_precision_args_t;
+
+constexpr int kMaxOrder = 100;   // Legendre::maxLegendreOrder
+constexpr int kRectangular = 0, kThin = 1, kFlat = 2, kFilament = 3;
+
+// ---------------------------------------------------------------------------
+// Segment blobs.  A field evaluation is a list of segments; each segment is one
+// coil's geometry plus a slice of its angular nodes and all of its thickness
+// (and length) nodes, laid out contiguously so one bulk copy stages it in
+// shared memory.  Segments are independent: the kernel converts each
+// segment's cylindrical partial sums to Cartesian and adds them to the point's
+// running total, so a coil whose node tables exceed one segment simply spans
+// several segments.
+// ---------------------------------------------------------------------------
+constexpr int kSegmentBytes = 16384;  // staging buffer per pipeline stage
+constexpr int kSegmentStages = 2;
+
+struct alignas(16) SegmentHeader
+{
+    double position[3];
+    double inv_transform[9];
+    double transform[9];
+    double half_length;   // b/2 (fast method)
+    double field_factor;  // 2 pi f for E, 1 otherwise
+    double inner_radius;  // R, for the on-axis test of the gradient
+    double near_r2;       // FP32 path: squared near-field radius around the winding (in the coil frame)
+    double near_lo[2];    // FP32 path: winding cross-section box {r_min, z_min} ...
+    double near_hi[2];    // ... and {r_max, z_max}
+    int n_t;              // thickness nodes
+    int n_l;              // length nodes (slow method)
+    int n_phi;            // angular nodes in this segment
+    int fast;             // 1 = analytic length integral (RECTANGULAR/THIN)
+    int off_t;            // table offsets in 16-byte units from the header start
+    int off_l;
+    int off_phi;
+    int off_f32;          // FP32 tables (0 when absent)
+};
+static_assert(sizeof(SegmentHeader) % 16 == 0, "segment header must keep 16-byte alignment");
+
+struct SegmentDesc
+{
+    long long offset;  // byte offset of the blob in the device buffer (multiple of 16)
+    int bytes;         // multiple of 16, <= kSegmentBytes
+    int coil;          // source coil index
+};
+
+// FP32 per-node tables appended after the FP64 tables (16 bytes per entry)
+struct alignas(16) PhiNode32
+{
+    float wc;    // w_phi * cos(phi), exactly antisymmetric over the mirror node
+    float omc;   // 1 - cos(phi) = 2 sin^2(phi/2)
+    float c;     // cos(phi)
+    float w;     // w_phi
+};
+
+// Host-built device tables for a coil set.
+struct SegmentSet
+{
+    std::vector<unsigned char> blob;  // host copy, 16-byte aligned entries
+    std::vector<SegmentDesc> segs;
+    int max_bytes = 0;
+};
+
+// Builds the segment list for `coils` (each at its own precision) for field
+// evaluation; precision selects whether FP32 tables are appended.
+bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err);
+
+// host_coil.cpp
+const double *legendreNodes(int order);
+const double *legendreWeights(int order);
+PrecisionArgs coilPrecision(const Coil &coil, double pf, int gpuCap);
+void pairPrecision(const Coil &prim, const Coil &sec, double pf, int gpuCap, bool zAxis, bool pureGPU,
+                   PrecisionArgs &primOut, PrecisionArgs &secOut);
+void initCoil(double R, double a, double b, int N, double I, double f, const double pos[3], double yAngle,
+              double zAngle, Coil &out);
+bool validArgs(const PrecisionArgs &p);
+
+// errors (thread-local message)
+void setError(const std::string &msg);
+int fail(int status, const std::string &msg);
+
+// kernels (fields.cu)
+struct FieldLaunch
+{
+    const unsigned char *d_blob;
+    const SegmentDesc *d_segs;
+    int nseg;
+    const double *d_points;
+    long long npts;
+    double *d_out;
+    int field;
+    int precision;
+    int lanes;
+};
+int launchFields(const FieldLaunch &L, void *stream);
+int readTimeouts(long long &count);
+} // namespace ccoil
+
+#endif

@@ -1,0 +1,514 @@
+// Field kernels: coils x points, Gauss-Legendre quadrature over each coil's
+// cross-section and azimuth, on CUDA cores (the integrand is transcendental,
+// there is no dense contraction for the tensor cores).
+//
+// Tiling.  A CTA owns a tile of points (blockDim / LANES points, LANES threads
+// per point) and walks the whole segment list.  Segment blobs (coil geometry +
+// node tables, see ccoil_internal.h) are staged into shared memory by the TMA
+// engine (cp.async.bulk, completion on an mbarrier), double buffered: while the
+// CTA integrates segment s, the bulk copy of segment s+1 is in flight.  All
+// threads read the same node at the same time (shared-memory broadcast).  The
+// LANES threads of a point split the angular nodes; each keeps Cartesian
+// accumulators and the LANES partial results are combined with warp shuffles
+// once, at the end.
+//
+// Integrands follow the reference's CPU code line for line in FP64:
+//   A fast  src/Coil/Fields/CalculateFieldsFast.cxx:13-83
+//   B fast  src/Coil/Fields/CalculateFieldsFast.cxx:85-160
+//   G fast  src/Coil/Fields/CalculateFieldsFast.cxx:162-266
+//   A/B/G slow  src/Coil/Fields/CalculateFieldsSlow.cxx:13-265
+//   Cartesian wrappers  src/Coil/Fields/CalculateFieldsMethods.cxx:6-84
+#include "ccoil_internal.h"
+
+#include <cuda_runtime.h>
+
+namespace ccoil
+{
+namespace
+{
+__device__ unsigned long long g_timeouts = 0;
+
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz: bounded mbarrier wait
+
+__device__ __forceinline__ unsigned smemAddr(const void *p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbarInit(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fenceBarrierInit()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Producer side: announce the byte count and start the bulk copy global -> shared.
+__device__ __forceinline__ void stageSegment(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbarTryWait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smemAddr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: returns false after ~2 s without completion.
+__device__ __forceinline__ bool mbarWait(unsigned long long *bar, unsigned parity)
+{
+    if (mbarTryWait(bar, parity))
+        return true;
+    long long start = clock64();
+    while (!mbarTryWait(bar, parity))
+    {
+        if (clock64() - start > kWaitCycles)
+            return false;
+    }
+    return true;
+}
+
+struct Frame
+{
+    double z, r, cphi, sphi;
+};
+
+// point -> coil frame cylindrical coordinates (CalculateFieldsMethods.cxx:8,
+// vec3::Vector3::getAsCylindricalCoords); cos/sin of atan2(y, x) as x/r, y/r
+__device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, double py, double pz)
+{
+    double dx = px - h.position[0], dy = py - h.position[1], dz = pz - h.position[2];
+    double x = h.inv_transform[0] * dx + h.inv_transform[1] * dy + h.inv_transform[2] * dz;
+    double y = h.inv_transform[3] * dx + h.inv_transform[4] * dy + h.inv_transform[5] * dz;
+    Frame f;
+    f.z = h.inv_transform[6] * dx + h.inv_transform[7] * dy + h.inv_transform[8] * dz;
+    f.r = sqrt(x * x + y * y);
+    if (f.r > 0.0)
+    {
+        double inv = 1.0 / f.r;
+        f.cphi = x * inv;
+        f.sphi = y * inv;
+    }
+    else
+    {
+        f.cphi = 1.0;  // atan2(0, 0) = 0
+        f.sphi = 0.0;
+    }
+    return f;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 segment integrals (cylindrical partial sums for one segment)
+// ---------------------------------------------------------------------------
+template <int LANES>
+__device__ __forceinline__ double segmentA64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                             const double2 *pt, const Frame &f, int lane)
+{
+    double sum = 0.0;
+    if (h.fast)
+    {
+        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            double2 t = tt[j];
+            double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r;
+            double part = 0.0;
+            for (int k = lane; k < h.n_phi; k += LANES)
+            {
+                double2 q = pt[k];
+                double g = rsqrt(cB - cA * q.x);
+                double d1 = top * g, d2 = bot * g;
+                double e1 = sqrt(d1 * d1 + 1.0), e2 = sqrt(d2 * d2 + 1.0);
+                part += q.y * q.x * log((e1 + d1) / (e2 + d2));
+            }
+            sum += t.y * t.x * part;
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            double2 l = lt[i];
+            double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                double2 t = tt[j];
+                double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r + zl * zl;
+                double part = 0.0;
+                for (int k = lane; k < h.n_phi; k += LANES)
+                {
+                    double2 q = pt[k];
+                    part += q.y * q.x * rsqrt(cB - cA * q.x);
+                }
+                sum += l.y * t.y * t.x * part;
+            }
+        }
+    }
+    return sum;
+}
+
+template <int LANES>
+__device__ __forceinline__ void segmentB64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                           const double2 *pt, const Frame &f, int lane, double &H, double &Z)
+{
+    H = 0.0;
+    Z = 0.0;
+    if (h.fast)
+    {
+        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            double2 t = tt[j];
+            double cA = t.x * t.x, cB = t.x * f.r, cC = cA + f.r * f.r;
+            double d1 = top * top + cC, d2 = bot * bot + cC;
+            double h0 = 0.0, z0 = 0.0;
+            for (int k = lane; k < h.n_phi; k += LANES)
+            {
+                double2 q = pt[k];
+                double F = 2.0 * cB * q.x;
+                double g1 = rsqrt(d1 - F), g2 = rsqrt(d2 - F);
+                h0 += q.y * q.x * (g2 - g1);
+                z0 += q.y * ((cA - 0.5 * F) / (cC - F)) * (top * g1 - bot * g2);
+            }
+            H += t.y * t.x * h0;
+            Z += t.y * z0;
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            double2 l = lt[i];
+            double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                double2 t = tt[j];
+                double cA = t.x * t.x, cB = t.x * zl, cC = t.x * f.r;
+                double cD = cA + f.r * f.r + zl * zl;
+                double h0 = 0.0, z0 = 0.0;
+                for (int k = lane; k < h.n_phi; k += LANES)
+                {
+                    double2 q = pt[k];
+                    double den = cD - 2.0 * cC * q.x;
+                    double g = q.y / (den * sqrt(den));
+                    z0 += g * (cA - cC * q.x);
+                    h0 += g * (cB * q.x);
+                }
+                double w = l.y * t.y;
+                H += w * h0;
+                Z += w * z0;
+            }
+        }
+    }
+}
+
+// {RPhi, RR, RZ, ZZ}
+template <int LANES>
+__device__ __forceinline__ void segmentG64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                           const double2 *pt, const Frame &f, int lane, double *g)
+{
+    double rphi = 0.0, rr = 0.0, rz = 0.0, zz = 0.0;
+    const double r = f.r;
+    if (h.fast)
+    {
+        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            double2 t = tt[j];
+            double A = t.x * t.x, B = r * r, C = t.x * r;
+            double D = A + B, E = A * A + B * B, F = C * C;
+            double G1 = D + top * top, G2 = D + bot * bot;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (int k = lane; k < h.n_phi; k += LANES)
+            {
+                double2 q = pt[k];
+                double c = q.x, c2 = c * c;
+                double pe = 2 * C * c;
+                double J1 = G1 - pe, J2 = G2 - pe;
+                double K1 = sqrt(J1), K2 = sqrt(J2);
+                double L1 = 1.0 / (J1 * K1), L2 = 1.0 / (J2 * K2);
+                double M = D - pe;
+                double N = 2 * F * c * (c2 + 2.0) - C * (3 * c2 + 1) * D + c * E;
+                double O = c * D - 2 * C;
+                double w = q.y;
+                s0 += w * (t.x * c / r) * (1.0 / K2 - 1.0 / K1);
+                s1 += w * (C - A * c) * c * (L1 - L2);
+                s3 += w * (A - C * c) * (L1 - L2);
+                s2 += w * t.x / (M * M) * (top * L1 * (O * J1 + N) - bot * L2 * (O * J2 + N));
+            }
+            rphi += t.y * s0;
+            rr += t.y * s1;
+            rz += t.y * s2;
+            zz += t.y * s3;
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            double2 l = lt[i];
+            double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                double2 t = tt[j];
+                double A = t.x * t.x, B = r * r, C = zl * zl;
+                double D = r * t.x, E = t.x * zl, F = 1.0 / r;
+                double G = 2.0 * A + 2.0 * B - C, Hh = A + B + C;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                for (int k = lane; k < h.n_phi; k += LANES)
+                {
+                    double2 q = pt[k];
+                    double c = q.x;
+                    double J = Hh - 2.0 * D * c;
+                    double sJ = sqrt(J);
+                    double X = q.y / (J * sJ);
+                    double Y = q.y / (J * J * sJ);
+                    s0 += X * (F * E * c);
+                    s1 += Y * (-3.0 * E * (r - t.x * c)) * c;
+                    s3 += Y * (-3.0 * E * (t.x - r * c));
+                    s2 += Y * (t.x * (G - D * c) * c - 3.0 * A * r);
+                }
+                double w = l.y * t.y;
+                rphi += w * s0;
+                rr += w * s1;
+                rz += w * s2;
+                zz += w * s3;
+            }
+        }
+    }
+    g[0] = rphi;
+    g[1] = rr;
+    g[2] = rz;
+    g[3] = zz;
+}
+
+// ---------------------------------------------------------------------------
+// Epilogues: cylindrical partials -> Cartesian, rotated by the coil transform,
+// added to the point's accumulators (linear in the partials, so per-lane
+// partials can be rotated before the cross-lane reduction).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void addRotated(const SegmentHeader &h, double vx, double vy, double vz, double *acc)
+{
+    acc[0] += h.transform[0] * vx + h.transform[1] * vy + h.transform[2] * vz;
+    acc[1] += h.transform[3] * vx + h.transform[4] * vy + h.transform[5] * vz;
+    acc[2] += h.transform[6] * vx + h.transform[7] * vy + h.transform[8] * vz;
+}
+
+// CalculateFieldsMethods.cxx:39-84, including the on-axis branch and the T*G
+// product of the reference.
+__device__ __forceinline__ void addGradient(const SegmentHeader &h, const Frame &f, const double *g, double *acc)
+{
+    double G[9];
+    double rphi = g[0], rr = g[1], rz = g[2], zz = g[3];
+    if (f.r / h.inner_radius < 1e-12)
+    {
+        G[0] = rr; G[1] = 0.0; G[2] = 0.0;
+        G[3] = 0.0; G[4] = rr; G[5] = 0.0;
+        G[6] = 0.0; G[7] = 0.0; G[8] = zz;
+    }
+    else
+    {
+        double c = f.cphi, s = f.sphi;
+        double xx = rr * c * c + rphi * s * s;
+        double yy = rr * s * s + rphi * c * c;
+        double xy = s * c * (rr - rphi);
+        double xz = rz * c, yz = rz * s;
+        G[0] = xx; G[1] = xy; G[2] = xz;
+        G[3] = xy; G[4] = yy; G[5] = yz;
+        G[6] = xz; G[7] = yz; G[8] = zz;
+    }
+    const double *T = h.transform;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            acc[3 * i + j] += T[3 * i] * G[j] + T[3 * i + 1] * G[3 + j] + T[3 * i + 2] * G[6 + j];
+}
+
+template <int FIELD, int LANES>
+__device__ __forceinline__ void integrateSegment64(const unsigned char *seg, double px, double py, double pz, int lane,
+                                                   double *acc)
+{
+    const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
+    const double2 *tt = reinterpret_cast<const double2 *>(seg) + h.off_t;
+    const double2 *lt = reinterpret_cast<const double2 *>(seg) + h.off_l;
+    const double2 *pt = reinterpret_cast<const double2 *>(seg) + h.off_phi;
+    Frame f = toCoilFrame(h, px, py, pz);
+    if (FIELD == CCOIL_FIELD_B)
+    {
+        double H, Z;
+        segmentB64<LANES>(h, tt, lt, pt, f, lane, H, Z);
+        addRotated(h, H * f.cphi, H * f.sphi, Z, acc);
+    }
+    else if (FIELD == CCOIL_FIELD_G)
+    {
+        double g[4];
+        segmentG64<LANES>(h, tt, lt, pt, f, lane, g);
+        addGradient(h, f, g, acc);
+    }
+    else
+    {
+        double a = segmentA64<LANES>(h, tt, lt, pt, f, lane) * h.field_factor;
+        addRotated(h, -a * f.sphi, a * f.cphi, 0.0, acc);
+    }
+}
+
+template <int FIELD, int LANES>
+__global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__restrict__ blob,
+                                                      const SegmentDesc *__restrict__ segs, int nseg,
+                                                      const double *__restrict__ points, long long npts,
+                                                      double *__restrict__ out)
+{
+    constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bars[kSegmentStages];
+
+    const int lane = threadIdx.x % LANES;
+    const long long p = (long long)blockIdx.x * (blockDim.x / LANES) + threadIdx.x / LANES;
+    const bool active = p < npts;
+
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kSegmentStages; ++s)
+            mbarInit(&bars[s], 1);
+        fenceBarrierInit();
+        for (int s = 0; s < kSegmentStages && s < nseg; ++s)
+            stageSegment(smem + s * kSegmentBytes, blob + segs[s].offset, (unsigned)segs[s].bytes, &bars[s]);
+    }
+    __syncthreads();
+
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (active)
+    {
+        px = points[3 * p];
+        py = points[3 * p + 1];
+        pz = points[3 * p + 2];
+    }
+    double acc[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i)
+        acc[i] = 0.0;
+
+    for (int s = 0; s < nseg; ++s)
+    {
+        const int stage = s % kSegmentStages;
+        const unsigned parity = (unsigned)((s / kSegmentStages) & 1);
+        bool ok = mbarWait(&bars[stage], parity);
+        if (__syncthreads_or(!ok))
+        {
+            if (threadIdx.x == 0)
+            {
+                atomicAdd(&g_timeouts, 1ull);
+                // let the copies still in flight land before the CTA exits: the
+                // newest segment issued into each stage is the largest j <= last
+                // with j % stages == stage
+                int last = min(s + kSegmentStages - 1, nseg - 1);
+                for (int t = 0; t < kSegmentStages; ++t)
+                {
+                    int j = last - ((last - t) % kSegmentStages + kSegmentStages) % kSegmentStages;
+                    if (j >= 0)
+                        mbarWait(&bars[t], (unsigned)((j / kSegmentStages) & 1));
+                }
+            }
+            return;
+        }
+        if (active)
+            integrateSegment64<FIELD, LANES>(smem + stage * kSegmentBytes, px, py, pz, lane, acc);
+        __syncthreads();
+        if (threadIdx.x == 0 && s + kSegmentStages < nseg)
+            stageSegment(smem + stage * kSegmentBytes, blob + segs[s + kSegmentStages].offset,
+                         (unsigned)segs[s + kSegmentStages].bytes, &bars[stage]);
+    }
+
+    // combine the LANES partial sums of each point (fixed order -> reproducible)
+#pragma unroll
+    for (int off = LANES / 2; off > 0; off /= 2)
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+    if (active && lane == 0)
+    {
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            out[W * p + i] = acc[i];
+    }
+}
+
+template <int FIELD>
+cudaError_t launch64(const FieldLaunch &L, cudaStream_t st)
+{
+    const int threads = 128;
+    const int ppb = threads / L.lanes;
+    long long blocks = (L.npts + ppb - 1) / ppb;
+    if (blocks > 2147483647LL)
+        return cudaErrorInvalidConfiguration;
+    size_t smem = (size_t)kSegmentStages * kSegmentBytes;
+    switch (L.lanes)
+    {
+#define CCOIL_CASE(N)                                                                                             \
+    case N:                                                                                                       \
+        fieldsKernel64<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(L.d_blob, L.d_segs, L.nseg, L.d_points, \
+                                                                          L.npts, L.d_out);                       \
+        break;
+        CCOIL_CASE(1)
+        CCOIL_CASE(2)
+        CCOIL_CASE(4)
+        CCOIL_CASE(8)
+        CCOIL_CASE(16)
+        CCOIL_CASE(32)
+#undef CCOIL_CASE
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+} // namespace
+
+int launchFields(const FieldLaunch &L, void *stream)
+{
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (L.npts == 0)
+        return CCOIL_OK;
+    if (L.nseg == 0)
+    {
+        int w = L.field == CCOIL_FIELD_G ? 9 : 3;
+        cudaError_t e = cudaMemsetAsync(L.d_out, 0, sizeof(double) * (size_t)L.npts * w, st);
+        return e == cudaSuccess ? CCOIL_OK : fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaError_t e;
+    switch (L.field)
+    {
+        case CCOIL_FIELD_A:
+        case CCOIL_FIELD_E: e = launch64<CCOIL_FIELD_A>(L, st); break;
+        case CCOIL_FIELD_B: e = launch64<CCOIL_FIELD_B>(L, st); break;
+        case CCOIL_FIELD_G: e = launch64<CCOIL_FIELD_G>(L, st); break;
+        default: return fail(CCOIL_ERR_INVALID_ARGUMENT, "unknown field");
+    }
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_CUDA, std::string("field kernel launch: ") + cudaGetErrorString(e));
+    return CCOIL_OK;
+}
+
+int readTimeouts(long long &count)
+{
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_timeouts, sizeof(v));
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+    count = (long long)v;
+    return CCOIL_OK;
+}
+} // namespace ccoil

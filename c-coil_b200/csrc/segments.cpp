@@ -1,0 +1,192 @@
+// Builds the per-coil node tables ("segments") that the field kernels stage
+// into shared memory.  The node positions and weights are those of the
+// reference's integrators:
+//   fast method: src/Coil/Fields/CalculateFieldsFast.cxx:17-55  (thickness x angle)
+//   slow method: src/Coil/Fields/CalculateFieldsSlow.cxx:17-66  (length x thickness x angle)
+// with the per-layer block subdivision of the reference, the overall constant
+// folded into the thickness weights, and the angular nodes on [0, pi]
+// (cosine is even, so the reference integrates half the turn and doubles it).
+#include "ccoil_internal.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace ccoil
+{
+namespace
+{
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kMuReduced = 1e-7;  // g_MiReduced
+
+struct Entry
+{
+    double a, b;
+};
+
+void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
+{
+    const unsigned char *c = static_cast<const unsigned char *>(p);
+    blob.insert(blob.end(), c, c + n);
+}
+} // namespace
+
+bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err)
+{
+    out.blob.clear();
+    out.segs.clear();
+    out.max_bytes = 0;
+    const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
+    const int perPhi = fp32 ? 32 : 16;  // bytes per angular node (FP64 entry + FP32 entry)
+
+    for (int ci = 0; ci < count; ++ci)
+    {
+        const Coil &k = coils[ci];
+        const PrecisionArgs &p = k.precision;
+        if (!validArgs(p))
+        {
+            err = "coil " + std::to_string(ci) + ": precision arguments out of range (increments 1..100, blocks >= 1)";
+            return false;
+        }
+        if (!(k.inner_radius > 0.0) || !(k.thickness > 0.0) || !(k.length > 0.0))
+        {
+            err = "coil " + std::to_string(ci) + ": inner radius, thickness and length must be positive";
+            return false;
+        }
+        const bool fast = k.use_fast_method != 0;
+
+        // thickness nodes with the overall constant folded in
+        const double tBlock = k.thickness / p.thickness_blocks;
+        const double aBlock = kPi / p.angular_blocks;
+        double constant;
+        if (fast)
+            constant = kMuReduced * k.current_density * tBlock * aBlock * 2 * 0.25;
+        else
+            constant = kMuReduced * k.current_density * (k.length / p.length_blocks) * tBlock * aBlock * 2 * 0.125;
+
+        std::vector<Entry> tNodes;
+        const double *tx = legendreNodes(p.thickness_increments), *tw = legendreWeights(p.thickness_increments);
+        for (int bt = 0; bt < p.thickness_blocks; ++bt)
+        {
+            double blockPos = k.inner_radius + tBlock * (bt + 0.5);
+            for (int i = 0; i < p.thickness_increments; ++i)
+                tNodes.push_back({blockPos + (tBlock * 0.5) * tx[i], constant * tw[i]});
+        }
+        std::vector<Entry> lNodes;
+        if (!fast)
+        {
+            const double lBlock = k.length / p.length_blocks;
+            const double *lx = legendreNodes(p.length_increments), *lw = legendreWeights(p.length_increments);
+            for (int bl = 0; bl < p.length_blocks; ++bl)
+            {
+                double blockPos = -k.length * 0.5 + lBlock * (bl + 0.5);
+                for (int i = 0; i < p.length_increments; ++i)
+                    lNodes.push_back({blockPos + (lBlock * 0.5) * lx[i], lw[i]});
+            }
+        }
+        // angular nodes over [0, pi]; cos(phi) = -sin(pi x / 2 ...) form is not
+        // used here: the FP64 tables follow the reference's cos(block centre + ...)
+        std::vector<Entry> phiNodes;
+        std::vector<PhiNode32> phi32;
+        const double *ax = legendreNodes(p.angular_increments), *aw = legendreWeights(p.angular_increments);
+        for (int bp = 0; bp < p.angular_blocks; ++bp)
+        {
+            double blockPos = aBlock * (bp + 0.5);
+            for (int i = 0; i < p.angular_increments; ++i)
+                phiNodes.push_back({std::cos(blockPos + (aBlock * 0.5) * ax[i]), aw[i]});
+        }
+        if (fp32)
+        {
+            // The FP32 tables use cos(phi) built to be exactly antisymmetric about
+            // pi/2 (node j and its mirror n-1-j), so the FP32 sum of w*cos over
+            // the nodes vanishes exactly, and 1 - cos(phi) from a half-angle sine
+            // (no cancellation near phi = 0).
+            const int n = (int)phiNodes.size();
+            phi32.resize(n);
+            for (int j = 0; j < n; ++j)
+            {
+                int bp = j / p.angular_increments, i = j % p.angular_increments;
+                double phi = aBlock * (bp + 0.5) + (aBlock * 0.5) * ax[i];
+                int m = n - 1 - j;  // mirror node
+                int mbp = m / p.angular_increments, mi = m % p.angular_increments;
+                double mphi = aBlock * (mbp + 0.5) + (aBlock * 0.5) * ax[mi];
+                // symmetric definition: c(j) = (cos(phi_j) - cos(phi_m)) / 2
+                double c = 0.5 * (std::cos(phi) - std::cos(mphi));
+                double s = std::sin(0.5 * phi);
+                float cf = (float)c;
+                phi32[j].c = cf;
+                phi32[j].w = (float)aw[i];
+                phi32[j].wc = (float)(aw[i] * c);
+                phi32[j].omc = (float)(2.0 * s * s);
+            }
+            for (int j = 0; j < n; ++j)
+            {
+                // force exact antisymmetry of the FP32 values
+                int m = n - 1 - j;
+                if (m < j)
+                {
+                    phi32[j].c = -phi32[m].c;
+                    phi32[j].wc = -phi32[m].wc;
+                }
+                else if (m == j)
+                {
+                    phi32[j].c = 0.0f;
+                    phi32[j].wc = 0.0f;
+                }
+            }
+        }
+
+        const int headerBytes = (int)sizeof(SegmentHeader);
+        const int fixedBytes = headerBytes + 16 * (int)(tNodes.size() + lNodes.size());
+        const int maxPhi = (kSegmentBytes - fixedBytes) / perPhi;
+        if (maxPhi < 1)
+        {
+            err = "coil " + std::to_string(ci) + ": thickness/length node tables exceed one staging segment";
+            return false;
+        }
+        const int nPhi = (int)phiNodes.size();
+        for (int start = 0; start < nPhi; start += maxPhi)
+        {
+            int cnt = std::min(maxPhi, nPhi - start);
+            SegmentHeader h;
+            std::memset(&h, 0, sizeof(h));
+            for (int i = 0; i < 3; ++i)
+                h.position[i] = k.position[i];
+            std::memcpy(h.inv_transform, k.inverse_transform, sizeof(h.inv_transform));
+            std::memcpy(h.transform, k.transform, sizeof(h.transform));
+            h.half_length = k.length * 0.5;
+            h.field_factor = field == CCOIL_FIELD_E ? 2 * kPi * k.sine_frequency : 1.0;
+            h.inner_radius = k.inner_radius;
+            h.n_t = (int)tNodes.size();
+            h.n_l = (int)lNodes.size();
+            h.n_phi = cnt;
+            h.fast = fast ? 1 : 0;
+            h.off_t = headerBytes / 16;
+            h.off_l = h.off_t + h.n_t;
+            h.off_phi = h.off_l + h.n_l;
+            h.off_f32 = fp32 ? h.off_phi + cnt : 0;
+            // near-field region of the FP32 path: the winding's cross-section box in
+            // (r, z), inflated by a margin; points inside go to the FP64 loop
+            double margin = std::max(std::max(k.thickness, k.length), 0.25 * k.inner_radius);
+            h.near_lo[0] = k.inner_radius - margin;
+            h.near_hi[0] = k.inner_radius + k.thickness + margin;
+            h.near_lo[1] = -0.5 * k.length - margin;
+            h.near_hi[1] = 0.5 * k.length + margin;
+            h.near_r2 = margin * margin;
+
+            SegmentDesc d;
+            d.offset = (long long)out.blob.size();
+            d.coil = ci;
+            appendBytes(out.blob, &h, sizeof(h));
+            appendBytes(out.blob, tNodes.data(), 16 * tNodes.size());
+            appendBytes(out.blob, lNodes.data(), 16 * lNodes.size());
+            appendBytes(out.blob, phiNodes.data() + start, 16 * (size_t)cnt);
+            if (fp32)
+                appendBytes(out.blob, phi32.data() + start, 16 * (size_t)cnt);
+            d.bytes = (int)(out.blob.size() - d.offset);
+            out.max_bytes = std::max(out.max_bytes, d.bytes);
+            out.segs.push_back(d);
+        }
+    }
+    return true;
+}
+} // namespace ccoil

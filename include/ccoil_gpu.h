@@ -1,0 +1,175 @@
+/*
+ * ccoil_gpu.h -- C-ABI of the B200 (sm_100a) field and coil-pair hot path of
+ * C-Coil.  Plain C types only: pointers, sizes, enums and POD structs.
+ *
+ * The library (libccoil_b200.so) replaces the reference's CUDA entry points
+ *   src/Coil/CUDAKernels/CoilAcceleration.h:8-29
+ *   src/CoilGroup/CUDAKernels/CoilGroupAcceleration.h:7-37
+ * and the host-side precision logic they depend on
+ *   src/Coil/PrecisionArguments/PrecisionArguments.cxx:57-288
+ *   src/Coil/PrecisionArguments/CoilPairArguments.cxx:20-255.
+ *
+ * Conventions
+ *   - Every entry point returns ccoil_status_t (0 = success) and never exits
+ *     the process.  ccoil_last_error_message() describes the last failure on
+ *     the calling thread.
+ *   - Points are interleaved xyz doubles (the memory layout of the reference's
+ *     vec3::Vector3Array).  Vector outputs are xyz doubles per point; gradient
+ *     outputs are 9 doubles per point in row-major order (xx xy xz yx ... zz),
+ *     the layout of vec3::Matrix3.
+ *   - `memory` says whether points/outputs are host pointers (the call copies
+ *     them and returns after the result is back in host memory) or device
+ *     pointers (the call is asynchronous on `stream`).  Coil descriptors are
+ *     always host memory.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *     stream).
+ */
+#ifndef CCOIL_GPU_H
+#define CCOIL_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCOIL_ABI_VERSION 1
+
+typedef enum ccoil_status
+{
+    CCOIL_OK = 0,
+    CCOIL_ERR_INVALID_ARGUMENT = 1,
+    CCOIL_ERR_CUDA = 2,
+    CCOIL_ERR_OUT_OF_MEMORY = 3,
+    CCOIL_ERR_NOT_SUPPORTED = 4,
+    CCOIL_ERR_TIMEOUT = 5,
+    CCOIL_ERR_NO_DEVICE = 6
+} ccoil_status_t;
+
+/* Arithmetic of the quadrature.  FP64 reproduces the reference's double CPU
+ * path; FP32_COMPENSATED runs the bulk of the nodes in FP32 with compensated
+ * accumulation and keeps FP64 for near-field points and the final sums. */
+typedef enum ccoil_precision
+{
+    CCOIL_PRECISION_FP64 = 0,
+    CCOIL_PRECISION_FP32_COMPENSATED = 1
+} ccoil_precision_t;
+
+typedef enum ccoil_field
+{
+    CCOIL_FIELD_A = 0, /* vector potential               (Coil::computeAllAPotentialVectors) */
+    CCOIL_FIELD_B = 1, /* magnetic flux density          (Coil::computeAllBFieldVectors)     */
+    CCOIL_FIELD_E = 2, /* electric field amplitude 2pi f A (Coil::computeAllEFieldVectors)   */
+    CCOIL_FIELD_G = 3  /* B gradient, T*G as the reference (Coil::computeAllBGradientMatrices) */
+} ccoil_field_t;
+
+typedef enum ccoil_memory
+{
+    CCOIL_MEMORY_HOST = 0,
+    CCOIL_MEMORY_DEVICE = 1
+} ccoil_memory_t;
+
+/* PrecisionArguments (src/Coil/Coil.h:47-94): blocks and Gauss-Legendre
+ * increments per layer (angular = phi, thickness = a, length = b). */
+typedef struct ccoil_precision_args
+{
+    int angular_blocks;
+    int thickness_blocks;
+    int length_blocks;
+    int angular_increments;
+    int thickness_increments;
+    int length_increments;
+} ccoil_precision_args_t;
+
+/* One coil as the reference's Coil object holds it (src/Coil/Coil.h:152-196):
+ * thin dimensions are already replaced by 1e-25*R (src/Coil/Coil.cxx:27-28),
+ * current_density = I*N/(a*b), transform/inverse_transform are the row-major
+ * matrices of Coil::calculateTransformationMatrices
+ * (src/Coil/Utils/CalculateAttributes.cxx:65-78). */
+typedef struct ccoil_coil
+{
+    double inner_radius;
+    double thickness;
+    double length;
+    double current_density;
+    double current;
+    double sine_frequency;
+    double position[3];
+    double y_axis_angle;
+    double z_axis_angle;
+    double transform[9];
+    double inverse_transform[9];
+    int num_turns;
+    int use_fast_method; /* RECTANGULAR/THIN: 1, FLAT/FILAMENT: 0 */
+    int coil_type;       /* 0 RECTANGULAR, 1 THIN, 2 FLAT, 3 FILAMENT (src/Coil/EnumsAndConstants/CoilType.h) */
+    ccoil_precision_args_t precision; /* precision used for this coil's fields */
+} ccoil_coil_t;
+
+/* Library identity. */
+int ccoil_abi_version(void);
+const char *ccoil_last_error_message(void);
+
+/* ------------------------------------------------------------------------ *
+ * Host-side mirrors of the reference's coil set-up and precision balancing  *
+ * ------------------------------------------------------------------------ */
+
+/* Coil::Coil(R, a, b, N, I, f, PrecisionFactor, threads, position, yAngle,
+ * zAngle) (src/Coil/Coil.cxx:46-67): fills `out` including the CPU precision
+ * arguments for precision_factor (gpu_increments == 0) or the GPU ones
+ * (gpu_increments = the reference's GPU_INCREMENTS cap). */
+int ccoil_coil_init(double inner_radius, double thickness, double length, int num_turns, double current,
+                    double sine_frequency, const double position[3], double y_axis_angle, double z_axis_angle,
+                    double precision_factor, int gpu_increments, ccoil_coil_t *out);
+
+/* PrecisionArguments::getCoilPrecisionArguments{CPU,GPU}
+ * (src/Coil/PrecisionArguments/PrecisionArguments.cxx:57-185);
+ * gpu_increments == 0 selects the CPU variant. */
+int ccoil_precision_arguments(const ccoil_coil_t *coil, double precision_factor, int gpu_increments,
+                              ccoil_precision_args_t *out);
+
+/* CoilPairArguments::getAppropriateCoilPairArguments
+ * (src/Coil/PrecisionArguments/CoilPairArguments.cxx:49-255);
+ * gpu_increments == 0 selects computeMethod != GPU. */
+int ccoil_pair_arguments(const ccoil_coil_t *primary, const ccoil_coil_t *secondary, double precision_factor,
+                         int gpu_increments, int z_axis_case, int pure_gpu, ccoil_precision_args_t *primary_out,
+                         ccoil_precision_args_t *secondary_out);
+
+/* Gauss-Legendre nodes and weights of order 1..100 in ascending node order
+ * (the content of src/LegendreMatrix/LegendreMatrix.cxx, computed). */
+int ccoil_legendre(int order, double *nodes, double *weights);
+
+/* ------------------------------------------------------------------------ *
+ * Fields of a coil or a coil group at many points                          *
+ * ------------------------------------------------------------------------ */
+
+/* Sum over `coil_count` coils of field `field` at `point_count` points, each
+ * coil at its own `precision` arguments.  coil_count == 1 is the single-coil
+ * path (Coil::computeAll*), coil_count > 1 the group path
+ * (CoilGroup::computeAll*).  Replaces Calculate_hardware_accelerated_{a,b,g}
+ * (src/Coil/CUDAKernels/CoilAcceleration.h:8-18) and
+ * Calculate_hardware_accelerated_{a,b,e,g}_group
+ * (src/CoilGroup/CUDAKernels/CoilGroupAcceleration.h:7-25). */
+int ccoil_compute_fields(const ccoil_coil_t *coils, int coil_count, const double *points, long long point_count,
+                         int field, int precision, double *out, int memory, void *stream);
+
+/* A prepared coil set: node tables built and resident in device memory, so
+ * repeated evaluations only move points and results. */
+typedef struct ccoil_field_plan ccoil_field_plan_t;
+
+int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field, int precision,
+                            ccoil_field_plan_t **plan);
+/* lanes_per_point: 0 = automatic, else 1, 2, 4, 8, 16 or 32 threads share one point. */
+int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, long long point_count, double *out,
+                             int memory, int lanes_per_point, void *stream);
+int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
+
+/* Number of device-side wait timeouts seen since the library was loaded (the
+ * bounded waits of the staging pipeline; a non-zero value also makes the
+ * failing call return CCOIL_ERR_TIMEOUT). */
+long long ccoil_timeout_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCOIL_GPU_H */
