@@ -1,0 +1,330 @@
+"""Benchmark of the field hot path on the coil-group workload.
+
+One step = A, B and G of a 128-coil mixed group (25% each RECTANGULAR, THIN,
+FLAT, FILAMENT; R ~ U[0.02, 0.3] m, a, b ~ U[0, 0.1] m, N ~ U{1..500},
+I ~ U[-5, 5] A, centres in a 1 m cube, random axes) at 2^20 points per GPU
+(uniform in a 2 m cube), PrecisionFactor 5, every coil at its CPU
+PrecisionArguments.  Seeded synthetic data; no dataset is involved.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32c|both]
+    python bench.py --impl reference        # the reference's own CPU_MT code on this host
+
+Under torchrun every rank evaluates its own 2^20 points (weak scaling, no
+collective on the data path); times are device times (CUDA events), max over
+ranks.  Rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "c-coil_b200"))
+
+METRIC = "coil-point field evals/s & M arrangements/s: FP32-comp vs FP64 at 1e-7 rel err"
+UNIT = "coil-point evals/s"
+FIELDS = (("A", 0), ("B", 1), ("G", 3))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c", "both"])
+    ap.add_argument("--points", type=int, default=1 << 20)
+    ap.add_argument("--coils", type=int, default=128)
+    ap.add_argument("--pf", type=float, default=5.0)
+    ap.add_argument("--cpu-sample-points", type=int, default=2048)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(a, world):
+    return {"workload": "coil group: %d mixed coils (RECT/THIN/FLAT/FILAMENT), %d points per GPU in a 2 m cube, "
+                        "A+B+G, PrecisionFactor %g" % (a.coils, a.points, a.pf),
+            "coils": a.coils, "points_per_gpu": a.points, "precision_factor": a.pf, "fields": ["A", "B", "G"],
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": "points sharded over %d rank(s), no data-path collective" % world}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU code (oracle/_ref), CPU_MT on all cores
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(a, sample_points):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+    from ccoil_b200 import workloads
+    cores = os.cpu_count() or 1
+    ref = Reference(threads=cores)
+    rows, _ = workloads.group_config(coils=a.coils, points=1)
+    pts = workloads.points_cube(sample_points, seed=1000 + 2)
+    t0 = time.perf_counter()
+    for _, f in FIELDS:
+        ref.group_fields(rows, pts, f, pf=a.pf, method=1)
+    dt = time.perf_counter() - t0
+    units = len(FIELDS) * a.coils * sample_points
+    return units / dt, cores, dt, "%d coils x %d points x A,B,G (CPU_MT, per-member MT path)" % (a.coils,
+                                                                                               sample_points)
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libccoil_ref.so was not built"}))
+        return
+    rates = []
+    sample = max(64, a.cpu_sample_points // 2)
+    for _ in range(a.warmup):
+        cpu_reference_rate(a, 64)
+    for _ in range(a.steps):
+        r, cores, dt, desc = cpu_reference_rate(a, sample)
+        rates.append((r, dt))
+    value = float(np.median([r for r, _ in rates]))
+    ms = float(np.mean([dt for _, dt in rates]) * 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": workload_config(a, world), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    COLS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+            "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.COLS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    import ccoil_b200 as cc
+    from ccoil_b200 import opcount, workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return float(x)
+        t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    rows, _ = workloads.group_config(coils=a.coils, points=1)
+    coils = workloads.coils_from_rows(rows, a.pf)
+    group = cc.CoilGroup(coils, cc.PrecisionFactor(a.pf))
+    pts_host = workloads.points_cube(a.points, seed=1000 + 2 + 7919 * rank)
+    pts = torch.from_numpy(pts_host).to(dev)
+    modes = {"fp64": [cc.PrecisionMode.FP64], "fp32c": [cc.PrecisionMode.FP32_COMPENSATED],
+             "both": [cc.PrecisionMode.FP64, cc.PrecisionMode.FP32_COMPENSATED]}[a.precision]
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    results = {}
+    for mode in modes:
+        plans = {name: group.plan(f, mode) for name, f in FIELDS}
+        outs = {name: torch.empty((a.points, 9 if f == 3 else 3), dtype=torch.float64, device=dev)
+                for name, f in FIELDS}
+        for _ in range(max(a.warmup, 3)):
+            for name, _f in FIELDS:
+                plans[name](pts, out=outs[name])
+        torch.cuda.synchronize()
+        field_ms = {name: 0.0 for name, _ in FIELDS}
+        step_ms = 0.0
+        barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            for _ in range(a.steps):
+                flush.fill_(1)  # evict L2 between steps (not timed)
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(FIELDS) + 1)]
+                ev[0].record()
+                for i, (name, _f) in enumerate(FIELDS):
+                    plans[name](pts, out=outs[name])
+                    ev[i + 1].record()
+                torch.cuda.synchronize()
+                for i, (name, _f) in enumerate(FIELDS):
+                    field_ms[name] += ev[i].elapsed_time(ev[i + 1])
+                step_ms += ev[0].elapsed_time(ev[-1])
+        torch.cuda.synchronize()
+        barrier()
+        step_ms = max_over_ranks(step_ms / a.steps)
+        field_ms = {k: max_over_ranks(v / a.steps) for k, v in field_ms.items()}
+        results[int(mode)] = {"step_ms": step_ms, "field_ms": field_ms, "clocks": clk.summary(),
+                              "outs": {k: v.clone() for k, v in outs.items()}}
+
+        # end to end through the public API: pinned host points in, pinned host results out
+        pin_pts = torch.from_numpy(pts_host).pin_memory()
+        pin_out = {name: torch.empty((a.points, 9 if f == 3 else 3), dtype=torch.float64).pin_memory()
+                   for name, f in FIELDS}
+        plans["A"](pin_pts.numpy(), out=pin_out["A"].numpy())  # warm the staging buffers
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            for name, _f in FIELDS:
+                plans[name](pin_pts.numpy(), out=pin_out[name].numpy())
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / a.steps)
+        results[int(mode)]["e2e_s"] = e2e_s
+        for p in plans.values():
+            p.close()
+
+    units_per_step = len(FIELDS) * a.coils * a.points * world
+    headline_mode = int(modes[-1])
+    r = results[headline_mode]
+    value = units_per_step / (r["step_ms"] * 1e-3)
+    e2e_value = units_per_step / r["e2e_s"]
+
+    # roofline of the dominant kernel against the measured pipe peak
+    p64, p32, pmu = (ctypes_peaks(cc) if rank == 0 else (None, None, None))
+    dom = max(r["field_ms"], key=r["field_ms"].get)
+    fidx = dict(FIELDS)[dom]
+    flops_launch = opcount.group_flops_per_point(fidx, coils) * a.points
+    achieved = flops_launch / (r["field_ms"][dom] * 1e-3) / 1e12
+    peak = p64 if headline_mode == 0 else p32
+    traffic = read_traffic(dom, headline_mode)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": r["step_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if headline_mode == 0 else "f32 (compensated) + f64",
+            "data": "synthetic (seeded)", "config": workload_config(a, world),
+            "precision_mode": "fp64" if headline_mode == 0 else "fp32c",
+            "per_field_ms": r["field_ms"],
+            "node_evals_per_s": opcount.group_nodes_per_point(coils) * a.points * world * len(FIELDS) /
+            (r["step_ms"] * 1e-3),
+            "gpu_launches": a.steps * len(FIELDS),
+            "clocks": r["clocks"],
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": len(FIELDS) * a.points * 24,
+                    "d2h_bytes_per_step": sum(a.points * 8 * (9 if f == 3 else 3) for _, f in FIELDS)},
+            "roofline": {"bound": "fp64-pipe" if headline_mode == 0 else "fp32-pipe+xu", "kernel": "field %s" % dom,
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                         "peak_source": "measured on this GPU by ccoil_measure_pipe_peaks (FMA = 2 flops)",
+                         "flops_per_launch": flops_launch,
+                         "pipes_measured": {"fp64_tflops": p64, "fp32_tflops": p32, "mufu_rsqrt_tops": pmu}}}
+    if len(modes) == 2:
+        r64 = results[0]
+        line["fp64"] = {"value": units_per_step / (r64["step_ms"] * 1e-3), "ms_per_step": r64["step_ms"],
+                        "per_field_ms": r64["field_ms"]}
+        line["fp32c_speedup_vs_fp64"] = r64["step_ms"] / r["step_ms"]
+        errs = {}
+        for name, f in FIELDS:
+            e = (results[1]["outs"][name] - r64["outs"][name]).norm(dim=1) / r64["outs"][name].norm(dim=1)
+            errs[name] = {"max": float(e.max()), "median": float(e.median())}
+        line["fp32c_rel_err_vs_fp64"] = errs
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        rate, cores, dt, desc = cpu_reference_rate(a, a.cpu_sample_points)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                                "sample": desc, "seconds": dt}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def ctypes_peaks(cc):
+    import ctypes
+    L = cc.lib()
+    L.ccoil_measure_pipe_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
+    v = [ctypes.c_double(), ctypes.c_double(), ctypes.c_double()]
+    if L.ccoil_measure_pipe_peaks(*[ctypes.byref(x) for x in v]) != 0:
+        return None, None, None
+    return v[0].value, v[1].value, v[2].value
+
+
+def read_traffic(field, mode):
+    """DRAM bytes per launch of the field kernel from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("%s_%s" % ("fp64" if mode == 0 else "fp32c", field))
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    main()

@@ -87,21 +87,24 @@ struct Frame
     double z, r, cphi, sphi;
 };
 
-// point -> coil frame cylindrical coordinates (CalculateFieldsMethods.cxx:8,
-// vec3::Vector3::getAsCylindricalCoords); cos/sin of atan2(y, x) as x/r, y/r
+// point -> coil frame cylindrical coordinates: inverse transform of (p - centre)
+// as vec3::Matrix3 * vec3::Vector3 evaluates it (Matrix3.cxx:50-55, left to right,
+// no fused multiply-add), then (z, sqrt(x^2 + y^2), atan2(y, x)) as
+// Vector3::getAsCylindricalCoords (Vector3.cxx:99-102); cos and sin of the
+// azimuth are taken as x/r and y/r
 __device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, double py, double pz)
 {
-    double dx = px - h.position[0], dy = py - h.position[1], dz = pz - h.position[2];
-    double x = h.inv_transform[0] * dx + h.inv_transform[1] * dy + h.inv_transform[2] * dz;
-    double y = h.inv_transform[3] * dx + h.inv_transform[4] * dy + h.inv_transform[5] * dz;
+    const double *M = h.inv_transform;
+    double dx = __dsub_rn(px, h.position[0]), dy = __dsub_rn(py, h.position[1]), dz = __dsub_rn(pz, h.position[2]);
+    double x = __dadd_rn(__dadd_rn(__dmul_rn(M[0], dx), __dmul_rn(M[1], dy)), __dmul_rn(M[2], dz));
+    double y = __dadd_rn(__dadd_rn(__dmul_rn(M[3], dx), __dmul_rn(M[4], dy)), __dmul_rn(M[5], dz));
     Frame f;
-    f.z = h.inv_transform[6] * dx + h.inv_transform[7] * dy + h.inv_transform[8] * dz;
-    f.r = sqrt(x * x + y * y);
+    f.z = __dadd_rn(__dadd_rn(__dmul_rn(M[6], dx), __dmul_rn(M[7], dy)), __dmul_rn(M[8], dz));
+    f.r = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
     if (f.r > 0.0)
     {
-        double inv = 1.0 / f.r;
-        f.cphi = x * inv;
-        f.sphi = y * inv;
+        f.cphi = x / f.r;
+        f.sphi = y / f.r;
     }
     else
     {
@@ -113,7 +116,20 @@ __device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, 
 
 // ---------------------------------------------------------------------------
 // FP64 segment integrals (cylindrical partial sums for one segment)
+//
+// Each node's value is computed with the reference's exact sequence of IEEE
+// double operations (round-to-nearest multiply/add/divide/sqrt, evaluated left
+// to right, no fused multiply-add), because several integrands cancel
+// catastrophically inside a node (e + d for d << 0 in A, G2 - G1 in B, the RZ
+// bracket of G): any other rounding would be amplified far above 1e-12 there.
+// Only the weighting and the accumulation are reassociated.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double sqr(double a) { return __dsqrt_rn(a); }
+
 template <int LANES>
 __device__ __forceinline__ double segmentA64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                              const double2 *pt, const Frame &f, int lane)
@@ -121,40 +137,45 @@ __device__ __forceinline__ double segmentA64(const SegmentHeader &h, const doubl
     double sum = 0.0;
     if (h.fast)
     {
-        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        // CalculateFieldsFast.cxx:27-78
+        const double top = add(f.z, h.half_length), bot = sub(f.z, h.half_length);
         for (int j = 0; j < h.n_t; ++j)
         {
-            double2 t = tt[j];
-            double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r;
+            const double2 t = tt[j];
+            const double cA = mul(mul(2.0, t.x), f.r);
+            const double cB = add(mul(t.x, t.x), mul(f.r, f.r));
             double part = 0.0;
             for (int k = lane; k < h.n_phi; k += LANES)
             {
-                double2 q = pt[k];
-                double g = rsqrt(cB - cA * q.x);
-                double d1 = top * g, d2 = bot * g;
-                double e1 = sqrt(d1 * d1 + 1.0), e2 = sqrt(d2 * d2 + 1.0);
-                part += q.y * q.x * log((e1 + d1) / (e2 + d2));
+                const double2 q = pt[k];
+                const double g = dvd(1.0, sqr(sub(cB, mul(cA, q.x))));
+                const double d1 = mul(top, g), d2 = mul(bot, g);
+                const double e1 = sqr(add(mul(d1, d1), 1.0)), e2 = sqr(add(mul(d2, d2), 1.0));
+                const double lg = log(dvd(add(e1, d1), add(e2, d2)));
+                part += mul(mul(q.y, q.x), lg);
             }
-            sum += t.y * t.x * part;
+            sum += mul(mul(t.y, t.x), part);
         }
     }
     else
     {
+        // CalculateFieldsSlow.cxx:55-78
         for (int i = 0; i < h.n_l; ++i)
         {
-            double2 l = lt[i];
-            double zl = l.x + f.z;
+            const double2 l = lt[i];
+            const double zl = add(l.x, f.z);
             for (int j = 0; j < h.n_t; ++j)
             {
-                double2 t = tt[j];
-                double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r + zl * zl;
+                const double2 t = tt[j];
+                const double cA = mul(mul(2.0, t.x), f.r);
+                const double cB = add(add(mul(t.x, t.x), mul(f.r, f.r)), mul(zl, zl));
                 double part = 0.0;
                 for (int k = lane; k < h.n_phi; k += LANES)
                 {
-                    double2 q = pt[k];
-                    part += q.y * q.x * rsqrt(cB - cA * q.x);
+                    const double2 q = pt[k];
+                    part += mul(q.y, dvd(mul(t.x, q.x), sqr(sub(cB, mul(cA, q.x)))));
                 }
-                sum += l.y * t.y * t.x * part;
+                sum += mul(mul(l.y, t.y), part);
             }
         }
     }
@@ -169,48 +190,52 @@ __device__ __forceinline__ void segmentB64(const SegmentHeader &h, const double2
     Z = 0.0;
     if (h.fast)
     {
-        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        // CalculateFieldsFast.cxx:100-155
+        const double top = add(f.z, h.half_length), bot = sub(f.z, h.half_length);
         for (int j = 0; j < h.n_t; ++j)
         {
-            double2 t = tt[j];
-            double cA = t.x * t.x, cB = t.x * f.r, cC = cA + f.r * f.r;
-            double d1 = top * top + cC, d2 = bot * bot + cC;
+            const double2 t = tt[j];
+            const double cA = mul(t.x, t.x), cB = mul(t.x, f.r);
+            const double cC = add(cA, mul(f.r, f.r));
+            const double d1 = add(mul(top, top), cC), d2 = add(mul(bot, bot), cC);
             double h0 = 0.0, z0 = 0.0;
             for (int k = lane; k < h.n_phi; k += LANES)
             {
-                double2 q = pt[k];
-                double F = 2.0 * cB * q.x;
-                double g1 = rsqrt(d1 - F), g2 = rsqrt(d2 - F);
-                h0 += q.y * q.x * (g2 - g1);
-                z0 += q.y * ((cA - 0.5 * F) / (cC - F)) * (top * g1 - bot * g2);
+                const double2 q = pt[k];
+                const double F = mul(mul(2.0, cB), q.x);
+                const double g1 = dvd(1.0, sqr(sub(d1, F))), g2 = dvd(1.0, sqr(sub(d2, F)));
+                h0 += mul(mul(q.y, q.x), sub(g2, g1));
+                z0 += mul(mul(q.y, dvd(sub(cA, mul(0.5, F)), sub(cC, F))), sub(mul(top, g1), mul(bot, g2)));
             }
-            H += t.y * t.x * h0;
-            Z += t.y * z0;
+            H += mul(mul(t.y, t.x), h0);
+            Z += mul(t.y, z0);
         }
     }
     else
     {
+        // CalculateFieldsSlow.cxx:129-158
         for (int i = 0; i < h.n_l; ++i)
         {
-            double2 l = lt[i];
-            double zl = l.x + f.z;
+            const double2 l = lt[i];
+            const double zl = add(l.x, f.z);
             for (int j = 0; j < h.n_t; ++j)
             {
-                double2 t = tt[j];
-                double cA = t.x * t.x, cB = t.x * zl, cC = t.x * f.r;
-                double cD = cA + f.r * f.r + zl * zl;
+                const double2 t = tt[j];
+                const double cA = mul(t.x, t.x), cB = mul(t.x, zl), cC = mul(t.x, f.r);
+                const double cD = add(add(cA, mul(f.r, f.r)), mul(zl, zl));
                 double h0 = 0.0, z0 = 0.0;
                 for (int k = lane; k < h.n_phi; k += LANES)
                 {
-                    double2 q = pt[k];
-                    double den = cD - 2.0 * cC * q.x;
-                    double g = q.y / (den * sqrt(den));
-                    z0 += g * (cA - cC * q.x);
-                    h0 += g * (cB * q.x);
+                    const double2 q = pt[k];
+                    const double F = mul(mul(2.0, cC), q.x);
+                    const double den = sub(cD, F);
+                    const double g = dvd(q.y, mul(den, sqr(den)));
+                    z0 += mul(g, sub(cA, mul(cC, q.x)));
+                    h0 += mul(g, mul(cB, q.x));
                 }
-                double w = l.y * t.y;
-                H += w * h0;
-                Z += w * z0;
+                const double w = mul(l.y, t.y);
+                H += mul(w, h0);
+                Z += mul(w, z0);
             }
         }
     }
@@ -225,68 +250,73 @@ __device__ __forceinline__ void segmentG64(const SegmentHeader &h, const double2
     const double r = f.r;
     if (h.fast)
     {
-        double top = f.z + h.half_length, bot = f.z - h.half_length;
+        // CalculateFieldsFast.cxx:179-254
+        const double top = add(f.z, h.half_length), bot = sub(f.z, h.half_length);
         for (int j = 0; j < h.n_t; ++j)
         {
-            double2 t = tt[j];
-            double A = t.x * t.x, B = r * r, C = t.x * r;
-            double D = A + B, E = A * A + B * B, F = C * C;
-            double G1 = D + top * top, G2 = D + bot * bot;
+            const double2 t = tt[j];
+            const double A = mul(t.x, t.x), B = mul(r, r), C = mul(t.x, r);
+            const double D = add(A, B), E = add(mul(A, A), mul(B, B)), F = mul(C, C);
+            const double G1 = add(D, mul(top, top)), G2 = add(D, mul(bot, bot));
             double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
             for (int k = lane; k < h.n_phi; k += LANES)
             {
-                double2 q = pt[k];
-                double c = q.x, c2 = c * c;
-                double pe = 2 * C * c;
-                double J1 = G1 - pe, J2 = G2 - pe;
-                double K1 = sqrt(J1), K2 = sqrt(J2);
-                double L1 = 1.0 / (J1 * K1), L2 = 1.0 / (J2 * K2);
-                double M = D - pe;
-                double N = 2 * F * c * (c2 + 2.0) - C * (3 * c2 + 1) * D + c * E;
-                double O = c * D - 2 * C;
-                double w = q.y;
-                s0 += w * (t.x * c / r) * (1.0 / K2 - 1.0 / K1);
-                s1 += w * (C - A * c) * c * (L1 - L2);
-                s3 += w * (A - C * c) * (L1 - L2);
-                s2 += w * t.x / (M * M) * (top * L1 * (O * J1 + N) - bot * L2 * (O * J2 + N));
+                const double2 q = pt[k];
+                const double c = q.x, c2 = mul(c, c);
+                const double pe = mul(mul(2.0, C), c);
+                const double J1 = sub(G1, pe), J2 = sub(G2, pe);
+                const double K1 = sqr(J1), K2 = sqr(J2);
+                const double L1 = dvd(1.0, mul(J1, K1)), L2 = dvd(1.0, mul(J2, K2));
+                const double M = sub(D, pe);
+                const double N = add(sub(mul(mul(mul(2.0, F), c), add(c2, 2.0)),
+                                         mul(mul(C, add(mul(3.0, c2), 1.0)), D)),
+                                     mul(c, E));
+                const double O = sub(mul(c, D), mul(2.0, C));
+                const double w = q.y;
+                s0 += mul(mul(w, dvd(mul(t.x, c), r)), sub(dvd(1.0, K2), dvd(1.0, K1)));
+                s1 += mul(mul(mul(w, sub(C, mul(A, c))), c), sub(L1, L2));
+                s3 += mul(mul(w, sub(A, mul(C, c))), sub(L1, L2));
+                s2 += mul(dvd(mul(w, t.x), mul(M, M)),
+                          sub(mul(mul(top, L1), add(mul(O, J1), N)), mul(mul(bot, L2), add(mul(O, J2), N))));
             }
-            rphi += t.y * s0;
-            rr += t.y * s1;
-            rz += t.y * s2;
-            zz += t.y * s3;
+            rphi += mul(t.y, s0);
+            rr += mul(t.y, s1);
+            rz += mul(t.y, s2);
+            zz += mul(t.y, s3);
         }
     }
     else
     {
+        // CalculateFieldsSlow.cxx:212-251
         for (int i = 0; i < h.n_l; ++i)
         {
-            double2 l = lt[i];
-            double zl = l.x + f.z;
+            const double2 l = lt[i];
+            const double zl = add(l.x, f.z);
             for (int j = 0; j < h.n_t; ++j)
             {
-                double2 t = tt[j];
-                double A = t.x * t.x, B = r * r, C = zl * zl;
-                double D = r * t.x, E = t.x * zl, F = 1.0 / r;
-                double G = 2.0 * A + 2.0 * B - C, Hh = A + B + C;
+                const double2 t = tt[j];
+                const double A = mul(t.x, t.x), B = mul(r, r), C = mul(zl, zl);
+                const double D = mul(r, t.x), E = mul(t.x, zl), F = dvd(1.0, r);
+                const double G = sub(add(mul(2.0, A), mul(2.0, B)), C), Hh = add(add(A, B), C);
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
                 for (int k = lane; k < h.n_phi; k += LANES)
                 {
-                    double2 q = pt[k];
-                    double c = q.x;
-                    double J = Hh - 2.0 * D * c;
-                    double sJ = sqrt(J);
-                    double X = q.y / (J * sJ);
-                    double Y = q.y / (J * J * sJ);
-                    s0 += X * (F * E * c);
-                    s1 += Y * (-3.0 * E * (r - t.x * c)) * c;
-                    s3 += Y * (-3.0 * E * (t.x - r * c));
-                    s2 += Y * (t.x * (G - D * c) * c - 3.0 * A * r);
+                    const double2 q = pt[k];
+                    const double c = q.x;
+                    const double J = sub(Hh, mul(mul(2.0, D), c));
+                    const double sJ = sqr(J);
+                    const double X = dvd(q.y, mul(J, sJ));
+                    const double Y = dvd(q.y, mul(mul(J, J), sJ));
+                    s0 += mul(X, mul(mul(F, E), c));
+                    s1 += mul(mul(Y, mul(-3.0, mul(E, sub(r, mul(t.x, c))))), c);
+                    s3 += mul(Y, mul(-3.0, mul(E, sub(t.x, mul(r, c)))));
+                    s2 += mul(Y, sub(mul(mul(t.x, sub(G, mul(D, c))), c), mul(mul(3.0, A), r)));
                 }
-                double w = l.y * t.y;
-                rphi += w * s0;
-                rr += w * s1;
-                rz += w * s2;
-                zz += w * s3;
+                const double w = mul(l.y, t.y);
+                rphi += mul(w, s0);
+                rr += mul(w, s1);
+                rz += mul(w, s2);
+                zz += mul(w, s3);
             }
         }
     }
@@ -295,7 +325,6 @@ __device__ __forceinline__ void segmentG64(const SegmentHeader &h, const double2
     g[2] = rz;
     g[3] = zz;
 }
-
 // ---------------------------------------------------------------------------
 // Epilogues: cylindrical partials -> Cartesian, rotated by the coil transform,
 // added to the point's accumulators (linear in the partials, so per-lane

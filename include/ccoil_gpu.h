@@ -168,6 +168,12 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
  * failing call return CCOIL_ERR_TIMEOUT). */
 long long ccoil_timeout_count(void);
 
+/* Diagnostic with no counterpart in the reference: measured throughput of the
+ * pipes that bound the field kernels on the current device -- FP64 FMA and
+ * FP32 FMA (TFLOP/s, an FMA counted as 2 flops) and MUFU reciprocal square
+ * root (tera-ops/s).  Used as roofline denominators. */
+int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops, double *mufu_tops);
+
 #ifdef __cplusplus
 }
 #endif
