@@ -48,14 +48,19 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
 
 
-def build(force=False, verbose=False, ptxas_info=False):
-    if not force and up_to_date():
+def build(force=False, verbose=False, ptxas_info=False, out=None, defines=()):
+    """Compile every source and link the library (out: alternative output path,
+    defines: extra -D macros for a variant build)."""
+    target = out or OUT
+    if not force and out is None and not defines and up_to_date():
         return OUT
-    os.makedirs(BUILD, exist_ok=True)
+    build_dir = BUILD if out is None and not defines else BUILD + "_variant"
+    os.makedirs(build_dir, exist_ok=True)
     objs = []
     for src in sources():
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
+        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-D" + d for d in defines] + ["-I", INCLUDE, "-I", CSRC, "-c", src,
+                                                                            "-o", obj]
         if src.endswith(".cpp"):
             cmd += ["-x", "cu"]
         if ptxas_info and src.endswith(".cu"):
@@ -69,14 +74,14 @@ def build(force=False, verbose=False, ptxas_info=False):
         if (verbose or ptxas_info) and (r.stdout or r.stderr):
             sys.stderr.write(r.stdout + r.stderr)
         objs.append(obj)
-    tmp = OUT + ".tmp"
+    tmp = target + ".tmp"
     cmd = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "shared"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
-    os.replace(tmp, OUT)
-    return OUT
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":
@@ -84,5 +89,8 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true")
+    ap.add_argument("--out", default=None, help="alternative output path")
+    ap.add_argument("-D", dest="defines", action="append", default=[], help="extra preprocessor macro")
     a = ap.parse_args()
-    print(build(force=a.force or a.ptxas_info, verbose=a.verbose, ptxas_info=a.ptxas_info))
+    print(build(force=a.force or a.ptxas_info, verbose=a.verbose, ptxas_info=a.ptxas_info, out=a.out,
+                defines=a.defines))

@@ -7,7 +7,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libccoil_b200.so")
+# CCOIL_B200_LIB selects another build of the same library (a variant build)
+LIB_PATH = os.environ.get("CCOIL_B200_LIB") or os.path.join(HERE, "libccoil_b200.so")
 
 CCOIL_OK = 0
 STATUS_NAMES = {

@@ -87,7 +87,7 @@ struct ccoil_field_plan
     int precision = 0;
     int coil_count = 0;
     SegmentSet set;
-    DeviceBuffer blob, segs, points, out;
+    DeviceBuffer blob, segs, points, out, work, workCount;
 };
 
 extern "C" {
@@ -158,8 +158,6 @@ int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field
         return fail(CCOIL_ERR_INVALID_ARGUMENT, "field must be A, B, E or G");
     if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
         return fail(CCOIL_ERR_INVALID_ARGUMENT, "precision must be FP64 or FP32_COMPENSATED");
-    if (precision == CCOIL_PRECISION_FP32_COMPENSATED)
-        return fail(CCOIL_ERR_NOT_SUPPORTED, "FP32_COMPENSATED fields are not built in this library version");
 
     ccoil_field_plan *p = new (std::nothrow) ccoil_field_plan();
     if (!p)
@@ -245,6 +243,24 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
     L.field = plan->field;
     L.precision = plan->precision;
     L.lanes = lanes_per_point ? lanes_per_point : autoLanes(point_count);
+    if (plan->precision == CCOIL_PRECISION_FP32_COMPENSATED)
+    {
+        // near-field work list: room for every (point, segment) pair up to 4 Mi
+        // entries (32 MiB); pairs beyond it are integrated in FP64 in place
+        unsigned long long want = (unsigned long long)point_count * (unsigned long long)L.nseg;
+        unsigned long long cap = want < (1ULL << 22) ? want : (1ULL << 22);
+        if (cap == 0)
+            cap = 1;
+        int rc0 = plan->work.reserve(cap * kNearPairBytes);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->workCount.reserve(sizeof(unsigned long long));
+        if (rc0 != CCOIL_OK)
+            return rc0;
+        L.d_work = plan->work.ptr;
+        L.work_capacity = plan->work.bytes / kNearPairBytes;
+        L.d_work_count = static_cast<unsigned long long *>(plan->workCount.ptr);
+        L.near_blocks = 148 * 8;
+    }
     int rc = launchFields(L, stream);
     if (rc != CCOIL_OK)
         return rc;
@@ -278,6 +294,8 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
     plan->segs.release();
     plan->points.release();
     plan->out.release();
+    plan->work.release();
+    plan->workCount.release();
     delete plan;
     return CCOIL_OK;
 }

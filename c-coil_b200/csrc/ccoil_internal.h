@@ -104,7 +104,13 @@ struct FieldLaunch
     int field;
     int precision;
     int lanes;
+    // FP32_COMPENSATED: near-field work list (scratch) and its counter
+    void *d_work = nullptr;                 // NearPair[work_capacity] (8 bytes each)
+    unsigned long long work_capacity = 0;
+    unsigned long long *d_work_count = nullptr;
+    int near_blocks = 0;                    // grid of the near-field pass
 };
+constexpr size_t kNearPairBytes = 8;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
 } // namespace ccoil

@@ -477,8 +477,10 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
     }
 }
 
+#include "fields32.cuh"
+
 template <int FIELD>
-cudaError_t launch64(const FieldLaunch &L, cudaStream_t st)
+cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
 {
     const int threads = 128;
     const int ppb = threads / L.lanes;
@@ -486,12 +488,18 @@ cudaError_t launch64(const FieldLaunch &L, cudaStream_t st)
     if (blocks > 2147483647LL)
         return cudaErrorInvalidConfiguration;
     size_t smem = (size_t)kSegmentStages * kSegmentBytes;
+    const bool fp32 = L.precision == CCOIL_PRECISION_FP32_COMPENSATED;
+    NearPair *work = reinterpret_cast<NearPair *>(L.d_work);
     switch (L.lanes)
     {
 #define CCOIL_CASE(N)                                                                                             \
     case N:                                                                                                       \
-        fieldsKernel64<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(L.d_blob, L.d_segs, L.nseg, L.d_points, \
-                                                                          L.npts, L.d_out);                       \
+        if (fp32)                                                                                                 \
+            fieldsKernel32<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(                                    \
+                L.d_blob, L.d_segs, L.nseg, L.d_points, L.npts, L.d_out, work, L.work_capacity, L.d_work_count);  \
+        else                                                                                                      \
+            fieldsKernel64<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(L.d_blob, L.d_segs, L.nseg,         \
+                                                                              L.d_points, L.npts, L.d_out);       \
         break;
         CCOIL_CASE(1)
         CCOIL_CASE(2)
@@ -502,6 +510,13 @@ cudaError_t launch64(const FieldLaunch &L, cudaStream_t st)
 #undef CCOIL_CASE
         default: return cudaErrorInvalidValue;
     }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !fp32)
+        return e;
+    // near-field pairs in FP64; the grid loops over the device-side count, so no
+    // host synchronisation is needed between the passes
+    nearFieldKernel<FIELD><<<L.near_blocks, 256, 0, st>>>(L.d_blob, L.d_segs, L.d_points, L.d_out, work,
+                                                            L.work_capacity, L.d_work_count);
     return cudaGetLastError();
 }
 } // namespace
@@ -518,12 +533,22 @@ int launchFields(const FieldLaunch &L, void *stream)
         return e == cudaSuccess ? CCOIL_OK : fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }
     cudaError_t e;
+    if (L.precision == CCOIL_PRECISION_FP32_COMPENSATED)
+    {
+        if (L.npts > 2147483647LL)
+            return fail(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED supports at most 2^31-1 points per call");
+        if (!L.d_work || !L.d_work_count)
+            return fail(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED needs a near-field work list");
+        e = cudaMemsetAsync(L.d_work_count, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess)
+            return fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+    }
     switch (L.field)
     {
         case CCOIL_FIELD_A:
-        case CCOIL_FIELD_E: e = launch64<CCOIL_FIELD_A>(L, st); break;
-        case CCOIL_FIELD_B: e = launch64<CCOIL_FIELD_B>(L, st); break;
-        case CCOIL_FIELD_G: e = launch64<CCOIL_FIELD_G>(L, st); break;
+        case CCOIL_FIELD_E: e = launchField<CCOIL_FIELD_A>(L, st); break;
+        case CCOIL_FIELD_B: e = launchField<CCOIL_FIELD_B>(L, st); break;
+        case CCOIL_FIELD_G: e = launchField<CCOIL_FIELD_G>(L, st); break;
         default: return fail(CCOIL_ERR_INVALID_ARGUMENT, "unknown field");
     }
     if (e != cudaSuccess)

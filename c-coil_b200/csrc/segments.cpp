@@ -9,6 +9,7 @@
 #include "ccoil_internal.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace ccoil
@@ -17,11 +18,26 @@ namespace
 {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kMuReduced = 1e-7;  // g_MiReduced
+constexpr double kDefaultNearMargin = 0.1;
 
 struct Entry
 {
     double a, b;
 };
+
+// Margin of the FP32 path's near-field box, as a multiple of the coil's inner
+// radius.  CCOIL_NEAR_MARGIN overrides it (a tuning knob read at plan creation).
+double nearMargin()
+{
+    const char *env = std::getenv("CCOIL_NEAR_MARGIN");
+    if (env)
+    {
+        double v = std::atof(env);
+        if (v >= 0.0 && v < 100.0)
+            return v;
+    }
+    return kDefaultNearMargin;
+}
 
 void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
 {
@@ -166,7 +182,7 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
             h.off_f32 = fp32 ? h.off_phi + cnt : 0;
             // near-field region of the FP32 path: the winding's cross-section box in
             // (r, z), inflated by a margin; points inside go to the FP64 loop
-            double margin = std::max(std::max(k.thickness, k.length), 0.25 * k.inner_radius);
+            double margin = nearMargin() * k.inner_radius;
             h.near_lo[0] = k.inner_radius - margin;
             h.near_hi[0] = k.inner_radius + k.thickness + margin;
             h.near_lo[1] = -0.5 * k.length - margin;

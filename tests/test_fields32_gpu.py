@@ -1,0 +1,107 @@
+"""FP32-compensated field path against the FP64 path (which reproduces the
+reference's double CPU results to 1e-12, see test_fields_gpu.py).
+
+Error is the norm-wise relative error per point.  Near-field (point, coil) pairs
+are evaluated with the FP64 integrands and must match the FP64 path exactly up
+to summation order; the gradient is compared outside its ill-conditioned band,
+where the FP64 reference form itself carries ~1e-7 rounding noise."""
+import numpy as np
+import pytest
+
+from conftest import gradient_band, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def modes(cc):
+    return cc.PrecisionMode.FP64, cc.PrecisionMode.FP32_COMPENSATED
+
+
+def evaluate(cc, coils, pts, field, mode, lanes=0):
+    plan = cc.FieldPlan([c.struct() for c in coils], field, mode)
+    try:
+        return plan(pts, lanes=lanes)
+    finally:
+        plan.close()
+
+
+@pytest.mark.parametrize("field", [0, 1, 2, 3])
+def test_group_workload_error(ccoil, field):
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(16, seed=77)
+    pts = workloads.points_cube(8192, seed=78)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    f64, f32 = (evaluate(ccoil, coils, pts, field, m) for m in modes(ccoil))
+    e = rel_err(f32, f64)
+    if field == 3:
+        e = e[~gradient_band(rows, pts)]
+    assert np.median(e) < 1e-7, np.median(e)
+    assert np.quantile(e, 0.99) < 5e-7, np.quantile(e, 0.99)
+    assert e.max() < 1e-5, e.max()
+
+
+def test_single_rect_workload_error(ccoil):
+    from ccoil_b200 import workloads
+    rows, pts = workloads.single_rect_config(points=16384, seed=3)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    for field in (0, 1, 3):
+        f64, f32 = (evaluate(ccoil, coils, pts, field, m) for m in modes(ccoil))
+        e = rel_err(f32, f64)
+        if field == 3:
+            e = e[~gradient_band(rows, pts)]
+        assert np.median(e) < 1e-7 and e.max() < 1e-5, (field, np.median(e), e.max())
+
+
+def test_near_field_pairs_use_fp64(ccoil):
+    # points inside the winding of a RECTANGULAR coil: every pair is near-field
+    coil = ccoil.Coil(0.1, 0.05, 0.08, 200)
+    rng = np.random.default_rng(5)
+    r = rng.uniform(0.1, 0.15, 2000)
+    ph = rng.uniform(0, 2 * np.pi, 2000)
+    z = rng.uniform(-0.04, 0.04, 2000)
+    pts = np.stack([r * np.cos(ph), r * np.sin(ph), z], axis=1)
+    for field in (0, 1, 3):
+        f64, f32 = (evaluate(ccoil, [coil], pts, field, m) for m in modes(ccoil))
+        assert rel_err(f32, f64).max() < 1e-13
+
+
+def test_work_list_overflow_falls_back_in_place(ccoil):
+    # 5 coincident coils x 2^20 points inside the winding = 5.2 Mi near-field pairs,
+    # more than the 4 Mi-entry work list: the rest is integrated in FP64 in place
+    coils = [ccoil.Coil(0.1, 0.02, 0.02, 10, precision_factor=1.0) for _ in range(5)]
+    n = 1 << 20
+    rng = np.random.default_rng(9)
+    r = rng.uniform(0.1, 0.12, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    z = rng.uniform(-0.01, 0.01, n)
+    pts = np.stack([r * np.cos(ph), r * np.sin(ph), z], axis=1)
+    f64, f32 = (evaluate(ccoil, coils, pts, 1, m) for m in modes(ccoil))
+    # inside the winding the 5 contributions nearly cancel; their FP64 atomic
+    # additions in either order agree to rounding level
+    assert rel_err(f32, f64).max() < 1e-12
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16, 32])
+def test_lane_splits(ccoil, lanes):
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(8, seed=11)
+    pts = workloads.points_cube(777, seed=12)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    for field in (0, 1, 3):
+        f64 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP64)
+        f32 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED, lanes)
+        e = rel_err(f32, f64)
+        if field == 3:
+            e = e[~gradient_band(rows, pts)]
+        assert np.median(e) < 1e-7 and e.max() < 1e-5, (field, lanes, e.max())
+
+
+def test_repeatable(ccoil):
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(8, seed=21)
+    pts = workloads.points_cube(4096, seed=22, half=0.6)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    a = evaluate(ccoil, coils, pts, 1, ccoil.PrecisionMode.FP32_COMPENSATED)
+    b = evaluate(ccoil, coils, pts, 1, ccoil.PrecisionMode.FP32_COMPENSATED)
+    # the near-field pass adds with FP64 atomics: run-to-run differences stay at rounding level
+    assert rel_err(a, b).max() < 1e-14
