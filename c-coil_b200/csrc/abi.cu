@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <cstring>
 #include <new>
 
@@ -12,7 +13,9 @@ namespace ccoil
 {
 namespace
 {
-thread_local std::string t_error;
+// last error message of the calling thread (fixed storage: reporting an error
+// never allocates)
+thread_local char t_error[512] = "";
 
 // Grow-only device buffer owned by a plan.
 struct DeviceBuffer
@@ -30,11 +33,13 @@ struct DeviceBuffer
 };
 } // namespace
 
-void setError(const std::string &msg) { t_error = msg; }
+void setError(const std::string &msg) { failMessage(CCOIL_OK, msg.c_str()); }
 
-int fail(int status, const std::string &msg)
+int fail(int status, const std::string &msg) { return failMessage(status, msg.c_str()); }
+
+int failMessage(int status, const char *msg)
 {
-    t_error = msg;
+    std::snprintf(t_error, sizeof(t_error), "%s", msg ? msg : "");
     return status;
 }
 
@@ -94,7 +99,7 @@ extern "C" {
 
 int ccoil_abi_version(void) { return CCOIL_ABI_VERSION; }
 
-const char *ccoil_last_error_message(void) { return t_error.c_str(); }
+const char *ccoil_last_error_message(void) { return t_error; }
 
 int ccoil_coil_init(double inner_radius, double thickness, double length, int num_turns, double current,
                     double sine_frequency, const double position[3], double y_axis_angle, double z_axis_angle,

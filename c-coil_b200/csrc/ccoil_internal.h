@@ -91,6 +91,7 @@ bool validArgs(const PrecisionArgs &p);
 // errors (thread-local message)
 void setError(const std::string &msg);
 int fail(int status, const std::string &msg);
+int failMessage(int status, const char *msg);  // same, without building a std::string
 
 // kernels (fields.cu)
 struct FieldLaunch

@@ -530,18 +530,18 @@ int launchFields(const FieldLaunch &L, void *stream)
     {
         int w = L.field == CCOIL_FIELD_G ? 9 : 3;
         cudaError_t e = cudaMemsetAsync(L.d_out, 0, sizeof(double) * (size_t)L.npts * w, st);
-        return e == cudaSuccess ? CCOIL_OK : fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+        return e == cudaSuccess ? CCOIL_OK : failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }
     cudaError_t e;
     if (L.precision == CCOIL_PRECISION_FP32_COMPENSATED)
     {
         if (L.npts > 2147483647LL)
-            return fail(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED supports at most 2^31-1 points per call");
+            return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED supports at most 2^31-1 points per call");
         if (!L.d_work || !L.d_work_count)
-            return fail(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED needs a near-field work list");
+            return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED needs a near-field work list");
         e = cudaMemsetAsync(L.d_work_count, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess)
-            return fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+            return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }
     switch (L.field)
     {
@@ -549,10 +549,10 @@ int launchFields(const FieldLaunch &L, void *stream)
         case CCOIL_FIELD_E: e = launchField<CCOIL_FIELD_A>(L, st); break;
         case CCOIL_FIELD_B: e = launchField<CCOIL_FIELD_B>(L, st); break;
         case CCOIL_FIELD_G: e = launchField<CCOIL_FIELD_G>(L, st); break;
-        default: return fail(CCOIL_ERR_INVALID_ARGUMENT, "unknown field");
+        default: return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown field");
     }
     if (e != cudaSuccess)
-        return fail(CCOIL_ERR_CUDA, std::string("field kernel launch: ") + cudaGetErrorString(e));
+        return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     return CCOIL_OK;
 }
 
