@@ -168,6 +168,25 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
  * failing call return CCOIL_ERR_TIMEOUT). */
 long long ccoil_timeout_count(void);
 
+/* FP32_COMPENSATED field evaluation that allocates nothing.  No counterpart in
+ * the reference.  For callers that cannot allocate device memory: code that
+ * runs while a CUDA graph is being captured, plugins inside a host program
+ * that owns every device allocation, real-time loops that must not stall.
+ * Same arguments and results as ccoil_compute_fields with precision
+ * FP32_COMPENSATED, except that `points` and `out` must be device pointers
+ * and the call is asynchronous on `stream`.
+ *
+ * Its scratch (node tables, segment list, near-field work list) is one fixed
+ * 3 MiB array in device memory, held by every GPU that loads the library until
+ * the process exits.  Limits: at most 1 MiB of node tables (about 400 coils at
+ * PrecisionFactor 5), 8192 segments and 2^31-1 points; larger requests return
+ * CCOIL_ERR_INVALID_ARGUMENT with a message.  The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams or host threads) race and must be ordered by the caller. */
+int ccoil_fields_fp32c_static(const ccoil_coil_t *coils, int coil_count, const double *points,
+                              long long point_count, int field, double *out, void *stream);
+
 /* Diagnostic with no counterpart in the reference: measured throughput of the
  * pipes that bound the field kernels on the current device -- FP64 FMA and
  * FP32 FMA (TFLOP/s, an FMA counted as 2 flops) and MUFU reciprocal square
