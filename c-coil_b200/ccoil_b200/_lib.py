@@ -41,6 +41,14 @@ class CoilStruct(ctypes.Structure):
                 ("precision", PrecisionArgsStruct)]
 
 
+class PoseStruct(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_double * 3), ("y_axis_angle", ctypes.c_double),
+                ("z_axis_angle", ctypes.c_double)]
+
+
+PAIR_MUTUAL_INDUCTANCE, PAIR_FORCE_TORQUE = 0, 1
+
+
 class CCoilError(RuntimeError):
     def __init__(self, status, message):
         super().__init__("ccoil status %s (%d): %s" % (STATUS_NAMES.get(status, "?"), status, message))
@@ -76,6 +84,8 @@ def lib():
     L.ccoil_field_plan_execute.argtypes = [vp, vp, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_int, vp]
     L.ccoil_field_plan_destroy.argtypes = [vp]
     L.ccoil_timeout_count.restype = ctypes.c_longlong
+    L.ccoil_pair_arrangements.argtypes = [cp, ctypes.c_int, cp, pp, vp, vp, ctypes.c_longlong, ctypes.c_int,
+                                          ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, vp]
     _lib = L
     return L
 

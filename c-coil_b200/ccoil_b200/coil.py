@@ -195,6 +195,34 @@ def _shape(res, field):
     return res
 
 
+def _poses(positions, y_angles, z_angles):
+    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+    y = np.ascontiguousarray(y_angles, dtype=np.float64).reshape(-1)
+    z = np.ascontiguousarray(z_angles, dtype=np.float64).reshape(-1)
+    if not (len(pos) == len(y) == len(z)):
+        raise ValueError("Array sizes do not match!")
+    return np.ascontiguousarray(np.concatenate([pos, y[:, None], z[:, None]], axis=1))
+
+
+def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity):
+    """Runs ccoil_pair_arrangements; returns (values, number of exact z-axis arrangements)."""
+    n = len(secondary_poses)
+    width = 1 if quantity == _lib.PAIR_MUTUAL_INDUCTANCE else 6
+    out = np.zeros((n, width))
+    prim = (_lib.CoilStruct * max(len(primaries), 1))(*primaries)
+    secp = (_lib.PrecisionArgsStruct * max(len(sec_precisions), 1))(*sec_precisions)
+    zc = ctypes.c_longlong(0)
+    check(lib().ccoil_pair_arrangements(
+        prim, len(primaries), ctypes.byref(secondary), secp,
+        None if primary_poses is None else primary_poses.ctypes.data_as(ctypes.c_void_p),
+        secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, _lib.PRECISION_FP64,
+        out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(zc), _lib.MEMORY_HOST, None))
+    return (out[:, 0] if width == 1 else out), zc.value
+
+
+_next_id = [0]
+
+
 class Coil:
     """Circular coil with rectangular cross-section (src/Coil/Coil.h:152-814).
 
@@ -208,6 +236,8 @@ class Coil:
                  z_axis_angle=0.0):
         self._args = (float(inner_radius), float(thickness), float(length), int(num_of_turns), float(current),
                       float(sine_frequency))
+        _next_id[0] += 1
+        self._id = _next_id[0]
         self.thread_count = thread_count
         self._pf = _factor(precision_factor if precision_factor is not None else PrecisionFactor())
         self._s = _lib.CoilStruct()
@@ -227,6 +257,7 @@ class Coil:
         return PrecisionArguments.from_struct(out)
 
     # --- getters mirroring the reference -------------------------------------------------
+    def get_id(self): return self._id
     def get_inner_radius(self): return self._s.inner_radius
     def get_thickness(self): return self._s.thickness
     def get_length(self): return self._s.length
@@ -285,6 +316,70 @@ class Coil:
     def compute_all_B_gradient_matrices(self, point_vectors, compute_method=ComputeMethod.GPU, used_precision=None,
                                         precision_mode=PrecisionMode.FP64):
         return self._compute(point_vectors, _lib.FIELD_G, compute_method, used_precision, precision_mode)
+
+    # --- coil pairs ------------------------------------------------------------------------
+    @staticmethod
+    def _pair_args(primary, secondary, pf):
+        """CPU pair arguments (computeMethod != GPU, general case), as the CPU path uses."""
+        a = CoilPairArguments.get_appropriate_coil_pair_arguments(primary, secondary, pf, ComputeMethod.CPU_ST)
+        return a.primary_precision, a.secondary_precision
+
+    @staticmethod
+    def _arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
+                      primary_z_angles, secondary_y_angles, secondary_z_angles, precision_factor, compute_method,
+                      quantity):
+        if ComputeMethod(compute_method) != ComputeMethod.GPU:
+            raise NotImplementedError("this package provides the ComputeMethod.GPU path only")
+        pp, sp = Coil._pair_args(primary, secondary, _factor(precision_factor))
+        ppose = _poses(primary_positions, primary_y_angles, primary_z_angles)
+        spose = _poses(secondary_positions, secondary_y_angles, secondary_z_angles)
+        if len(ppose) != len(spose):
+            raise ValueError("Array sizes do not match!")
+        vals, _ = _pair_arrangements([primary.struct(pp)], secondary.struct(sp), [sp.to_struct()], ppose, spose,
+                                     quantity)
+        return vals
+
+    @staticmethod
+    def compute_all_mutual_inductance_arrangements(primary, secondary, primary_positions, secondary_positions,
+                                                   primary_y_angles, primary_z_angles, secondary_y_angles,
+                                                   secondary_z_angles, precision_factor=None,
+                                                   compute_method=ComputeMethod.GPU):
+        """Coil::computeAllMutualInductanceArrangements (ComputeMInductanceMethods.cxx:200-260): (n,) array."""
+        return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
+                                  primary_z_angles, secondary_y_angles, secondary_z_angles,
+                                  precision_factor or PrecisionFactor(), compute_method,
+                                  _lib.PAIR_MUTUAL_INDUCTANCE)
+
+    @staticmethod
+    def compute_all_force_torque_arrangements(primary, secondary, primary_positions, secondary_positions,
+                                              primary_y_angles, primary_z_angles, secondary_y_angles,
+                                              secondary_z_angles, precision_factor=None,
+                                              compute_method=ComputeMethod.GPU):
+        """Coil::computeAllForceTorqueArrangements (ComputeForceMethods.cxx:189-248): (n, 6) array of
+        force xyz and torque xyz on the secondary."""
+        return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
+                                  primary_z_angles, secondary_y_angles, secondary_z_angles,
+                                  precision_factor or PrecisionFactor(), compute_method, _lib.PAIR_FORCE_TORQUE)
+
+    def _pose_row(self):
+        return self.get_position_vector(), self._s.y_axis_angle, self._s.z_axis_angle
+
+    @staticmethod
+    def compute_mutual_inductance(primary, secondary, precision_factor=None, compute_method=ComputeMethod.GPU):
+        """Coil::computeMutualInductance for the pair as placed (general case)."""
+        pp, py, pz = primary._pose_row()
+        sp, sy, sz = secondary._pose_row()
+        return float(Coil.compute_all_mutual_inductance_arrangements(
+            primary, secondary, [pp], [sp], [py], [pz], [sy], [sz], precision_factor, compute_method)[0])
+
+    @staticmethod
+    def compute_force_torque(primary, secondary, precision_factor=None, compute_method=ComputeMethod.GPU):
+        """Coil::computeForceTorque for the pair as placed: (force xyz, torque xyz)."""
+        pp, py, pz = primary._pose_row()
+        sp, sy, sz = secondary._pose_row()
+        v = Coil.compute_all_force_torque_arrangements(primary, secondary, [pp], [sp], [py], [pz], [sy], [sz],
+                                                       precision_factor, compute_method)[0]
+        return v[:3].copy(), v[3:].copy()
 
     def __repr__(self):
         R, a, b, N, I, f = self._args
@@ -355,6 +450,48 @@ class CoilGroup:
     def compute_all_B_gradient_matrices(self, point_vectors, compute_method=ComputeMethod.GPU,
                                         precision_mode=PrecisionMode.FP64):
         return self._compute(point_vectors, _lib.FIELD_G, compute_method, precision_mode)
+
+    # --- coil pairs: the secondary against every member except itself ---------------------
+    def _group_arrangements(self, secondary, positions, y_angles, z_angles, precision_factor, compute_method,
+                            quantity):
+        if ComputeMethod(compute_method) != ComputeMethod.GPU:
+            raise NotImplementedError("this package provides the ComputeMethod.GPU path only")
+        pf = _factor(precision_factor or PrecisionFactor())
+        prims, secs = [], []
+        for m in self.member_coils:
+            if m.get_id() == secondary.get_id():
+                continue  # CoilGroup::computeMutualInductance skips the secondary (ComputeMInductance.cxx:15)
+            pp, sp = Coil._pair_args(m, secondary, pf)
+            prims.append(m.struct(pp))
+            secs.append(sp.to_struct())
+        spose = _poses(positions, y_angles, z_angles)
+        vals, _ = _pair_arrangements(prims, secondary.struct(), secs, None, spose, quantity)
+        return vals
+
+    def compute_all_mutual_inductance_arrangements(self, secondary, secondary_positions, secondary_y_angles,
+                                                   secondary_z_angles, precision_factor=None,
+                                                   compute_method=ComputeMethod.GPU):
+        """CoilGroup::computeAllMutualInductanceArrangements (ComputeMInductance.cxx:23-64)."""
+        return self._group_arrangements(secondary, secondary_positions, secondary_y_angles, secondary_z_angles,
+                                        precision_factor, compute_method, _lib.PAIR_MUTUAL_INDUCTANCE)
+
+    def compute_all_force_torque_arrangements(self, secondary, secondary_positions, secondary_y_angles,
+                                              secondary_z_angles, precision_factor=None,
+                                              compute_method=ComputeMethod.GPU):
+        """CoilGroup::computeAllForceTorqueArrangements (ComputeForce.cxx:47-89): (n, 6)."""
+        return self._group_arrangements(secondary, secondary_positions, secondary_y_angles, secondary_z_angles,
+                                        precision_factor, compute_method, _lib.PAIR_FORCE_TORQUE)
+
+    def compute_mutual_inductance(self, secondary, precision_factor=None, compute_method=ComputeMethod.GPU):
+        p, y, z = secondary._pose_row()
+        return float(self.compute_all_mutual_inductance_arrangements(secondary, [p], [y], [z], precision_factor,
+                                                                     compute_method)[0])
+
+    def compute_force_torque(self, secondary, precision_factor=None, compute_method=ComputeMethod.GPU):
+        p, y, z = secondary._pose_row()
+        v = self.compute_all_force_torque_arrangements(secondary, [p], [y], [z], precision_factor,
+                                                       compute_method)[0]
+        return v[:3].copy(), v[3:].copy()
 
 
 def legendre(order):

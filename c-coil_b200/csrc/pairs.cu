@@ -1,0 +1,496 @@
+// Coil-pair kernels: mutual inductance and force/torque over many arrangements
+// (the reference's CPU general case, evaluated for every arrangement at once).
+//
+// Reference algorithm per arrangement and primary (CPU path):
+//   Coil::calculateMutualInductanceGeneral  src/Coil/MInductance/CalculateMInductanceGeneral.cxx:8-117
+//   Coil::calculateForceTorqueGeneral       src/Coil/ForceAndTorque/CalculateForceGeneral.cxx:9-131
+//   ring nodes  Coil::calculateRingIncrementPosition  src/Coil/Utils/SupportFunctions.cxx:72-122
+//   coplanar axes  Coil::improvedPrecisionCase       src/Coil/Utils/SupportFunctions.cxx:124-161
+//   group sums  CoilGroup::computeMutualInductance / computeForceTorque
+//               src/CoilGroup/MInductance/ComputeMInductance.cxx:4-20,
+//               src/CoilGroup/ForceAndTorque/ComputeForce.cxx:4-28
+// The secondary is a cloud of nodes (length x thickness x azimuth); at each
+// node the primary's A (for M) or B (for F/T) is the full FP64 field quadrature
+// of integrands64.cuh.
+//
+// Mapping.  One warp per arrangement (grid-stride); the 32 lanes split the
+// secondary's nodes, each lane evaluates the primary's whole quadrature at its
+// node; the node tables are read from global memory (all lanes read the same
+// primary node: L1 broadcast).  A fixed-order shuffle reduction per primary
+// gives a deterministic result; primaries of a group are summed in order.
+#include "ccoil_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace ccoil
+{
+namespace
+{
+#include "integrands64.cuh"
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kMuReduced = 1e-7;
+
+// One primary of a pair, followed in the blob by its tables.
+struct alignas(16) PairHeader
+{
+    SegmentHeader prim;  // primary geometry (its own pose, used when primaries do not move) and node counts
+    double m_factor;     // 2 pi N2 / (I1 lB tB aB): mutual inductance scale
+    double f_factor;     // 2 pi I2 N2 / (lB tB aB): force/torque scale
+    double prim_y_angle; // the primary's own orientation (used when primaries do not move)
+    double prim_z_angle;
+    int s_nl, s_nt, s_na, s_ablocks;  // secondary node counts and angular blocks
+    int off_sl, off_st, off_sa, pad2; // secondary tables (16-byte units from the header)
+};
+static_assert(sizeof(PairHeader) % 16 == 0, "pair header alignment");
+
+struct alignas(16) SecAngular
+{
+    double bpos;  // angular block index + 0.5
+    double x;     // Gauss-Legendre node in [-1, 1]
+    double w;     // its weight
+    double pad;
+};
+
+struct Pose
+{
+    double pos[3];
+    double T[9];
+    double Ti[9];
+};
+
+// Coil::calculateTransformationMatrices (src/Coil/Utils/CalculateAttributes.cxx:65-78)
+__device__ __forceinline__ void poseFromAngles(const double *p, Pose &o)
+{
+    o.pos[0] = p[0];
+    o.pos[1] = p[1];
+    o.pos[2] = p[2];
+    double sY, cY, sZ, cZ;
+    sincos(p[3], &sY, &cY);
+    sincos(p[4], &sZ, &cZ);
+    o.T[0] = cZ * cZ * cY - sZ * sZ;  o.T[1] = -sZ * cZ * cY - sZ * cZ;  o.T[2] = cZ * sY;
+    o.T[3] = sZ * cZ * cY + sZ * cZ;  o.T[4] = cZ * cZ - sZ * sZ * cY;   o.T[5] = sZ * sY;
+    o.T[6] = -sY * cZ;                o.T[7] = sY * sZ;                  o.T[8] = cY;
+    o.Ti[0] = cZ * cZ * cY - sZ * sZ; o.Ti[1] = sZ * cZ * cY + sZ * cZ;  o.Ti[2] = -cZ * sY;
+    o.Ti[3] = -sZ * cZ * cY - sZ * cZ; o.Ti[4] = cZ * cZ - sZ * sZ * cY; o.Ti[5] = sZ * sY;
+    o.Ti[6] = sY * cZ;                o.Ti[7] = sY * sZ;                 o.Ti[8] = cY;
+}
+
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *o)
+{
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// improvedPrecisionCase: when the two axes and the centre offset are coplanar
+// the reference integrates half of the secondary ring starting at `offset`
+__device__ __forceinline__ bool improvedCase(const double *pp, const double *sp, double &offset)
+{
+    const double pn[3] = {sin(pp[3]) * cos(pp[4]), sin(pp[3]) * sin(pp[4]), cos(pp[3])};
+    const double sn[3] = {sin(sp[3]) * cos(sp[4]), sin(sp[3]) * sin(sp[4]), cos(sp[3])};
+    const double d[3] = {pp[0] - sp[0], pp[1] - sp[1], pp[2] - sp[2]};
+    double pl[3];
+    cross3(pn, d, pl);
+    const double dot = pl[0] * sn[0] + pl[1] * sn[1] + pl[2] * sn[2];
+    offset = 0.0;
+    if (!(fabs(dot) <= 1e-14))
+        return false;
+    if (pl[0] == 0.0 && pl[1] == 0.0 && pl[2] == 0.0)
+        cross3(sn, d, pl);
+    if (pl[0] == 0.0 && pl[1] == 0.0 && pl[2] == 0.0)
+        cross3(sn, pn, pl);
+    offset = atan2(cos(sp[3]) * (pl[0] * cos(sp[4]) + pl[1] * sin(sp[4])) - pl[2] * sin(sp[3]),
+                   pl[0] * sin(sp[4]) - pl[1] * cos(sp[4]));
+    return true;
+}
+
+// Coil::isZAxisCase (src/Coil/Utils/SupportFunctions.cxx:55-70)
+__device__ __forceinline__ bool zAxisCase(const double *pp, const double *sp, double primR)
+{
+    return fabs(pp[0] / primR) < 1e-12 && fabs(pp[1] / primR) < 1e-12 && fabs(sp[0] / primR) < 1e-12 &&
+           fabs(sp[1] / primR) < 1e-12 && fabs(pp[3] / (2 * kPi)) < 1e-12 && fabs(sp[3] / (2 * kPi)) < 1e-12;
+}
+
+__device__ __forceinline__ Frame frameAt(const Pose &P, const double *q)
+{
+    SegmentHeader h;  // only position / inverse transform are read
+    for (int i = 0; i < 3; ++i)
+        h.position[i] = P.pos[i];
+    for (int i = 0; i < 9; ++i)
+        h.inv_transform[i] = P.Ti[i];
+    return toCoilFrame(h, q[0], q[1], q[2]);
+}
+
+template <int QTY>
+__global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restrict__ blob,
+                                                    const long long *__restrict__ primOffsets, int nprim,
+                                                    const double *__restrict__ primPoses,
+                                                    const double *__restrict__ secPoses, long long count,
+                                                    double *__restrict__ out,
+                                                    unsigned long long *__restrict__ zAxisCount)
+{
+    constexpr int W = QTY == 0 ? 1 : 6;
+    const int lane = threadIdx.x % 32;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const long long warps = (long long)gridDim.x * blockDim.x / 32;
+    for (long long a = warp; a < count; a += warps)
+    {
+        const double *sp = secPoses + 5 * a;
+        double sA, cA, sB, cB;
+        sincos(sp[3], &sA, &cA);
+        sincos(sp[4], &sB, &cB);
+        double total[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            total[i] = 0.0;
+        for (int j = 0; j < nprim; ++j)
+        {
+            const unsigned char *base = blob + primOffsets[j];
+            const PairHeader &ph = *reinterpret_cast<const PairHeader *>(base);
+            const SegmentHeader &h = ph.prim;
+            const double2 *tt = reinterpret_cast<const double2 *>(base) + h.off_t;
+            const double2 *lt = reinterpret_cast<const double2 *>(base) + h.off_l;
+            const double2 *pt = reinterpret_cast<const double2 *>(base) + h.off_phi;
+            const double2 *sl = reinterpret_cast<const double2 *>(base) + ph.off_sl;
+            const double2 *st = reinterpret_cast<const double2 *>(base) + ph.off_st;
+            const SecAngular *sa = reinterpret_cast<const SecAngular *>(reinterpret_cast<const double2 *>(base) +
+                                                                        ph.off_sa);
+            Pose P;
+            double ppose[5];
+            if (primPoses)
+            {
+                for (int i = 0; i < 5; ++i)
+                    ppose[i] = primPoses[5 * a + i];
+                poseFromAngles(ppose, P);
+            }
+            else
+            {
+                for (int i = 0; i < 3; ++i)
+                    P.pos[i] = ppose[i] = h.position[i];
+                for (int i = 0; i < 9; ++i)
+                {
+                    P.T[i] = h.transform[i];
+                    P.Ti[i] = h.inv_transform[i];
+                }
+                ppose[3] = ph.prim_y_angle;
+                ppose[4] = ph.prim_z_angle;
+            }
+            if (lane == 0 && zAxisCount && zAxisCase(ppose, sp, h.inner_radius))
+                atomicAdd(zAxisCount, 1ull);
+            double offset = 0.0;
+            const bool improved = QTY == 0 ? improvedCase(ppose, sp, offset) : false;
+            const double ablk = (improved ? kPi : 2 * kPi) / ph.s_ablocks;
+            const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
+            double part[W];
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                part[i] = 0.0;
+            for (int n = lane; n < nsec; n += 32)
+            {
+                const int k = n % ph.s_na, lt_i = n / ph.s_na;
+                const int t = lt_i % ph.s_nt, l = lt_i / ph.s_nt;
+                const double2 L = sl[l], R = st[t];
+                const SecAngular A = sa[k];
+                const double phi = (offset + ablk * A.bpos) + (ablk * 0.5) * A.x;
+                double sP, cP;
+                sincos(phi, &sP, &cP);
+                const double ringP[3] = {cB * cA * cP - sB * sP, sB * cA * cP + cB * sP, -sA * cP};
+                const double tan[3] = {-cB * cA * sP - sB * cP, -sB * cA * sP + cB * cP, sA * sP};
+                const double q[3] = {sp[0] + L.x * sA * cB + R.x * ringP[0], sp[1] + L.x * sA * sB + R.x * ringP[1],
+                                     sp[2] + L.x * cA + R.x * ringP[2]};
+                const double w = 0.125 * R.x * L.y * R.y * A.w;
+                const Frame f = frameAt(P, q);
+                if (QTY == 0)
+                {
+                    const double av = segmentA64<1>(h, tt, lt, pt, f, 0);
+                    const double vx = -av * f.sphi, vy = av * f.cphi;
+                    const double Ax = P.T[0] * vx + P.T[1] * vy, Ay = P.T[3] * vx + P.T[4] * vy,
+                                 Az = P.T[6] * vx + P.T[7] * vy;
+                    part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
+                }
+                else
+                {
+                    double H, Z;
+                    segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
+                    const double vx = H * f.cphi, vy = H * f.sphi;
+                    const double B[3] = {P.T[0] * vx + P.T[1] * vy + P.T[2] * Z, P.T[3] * vx + P.T[4] * vy + P.T[5] * Z,
+                                         P.T[6] * vx + P.T[7] * vy + P.T[8] * Z};
+                    double dF[3], dT[3];
+                    cross3(tan, B, dF);
+                    for (int i = 0; i < 3; ++i)
+                        dF[i] *= w;
+                    const double rel[3] = {q[0] - sp[0], q[1] - sp[1], q[2] - sp[2]};
+                    cross3(rel, dF, dT);
+                    for (int i = 0; i < 3; ++i)
+                    {
+                        part[i] += dF[i];
+                        part[3 + i] += dT[i];
+                    }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off /= 2)
+#pragma unroll
+                for (int i = 0; i < W; ++i)
+                    part[i] += __shfl_xor_sync(0xffffffffu, part[i], off);
+            const double scale = QTY == 0 ? ph.m_factor : ph.f_factor;
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                total[i] += part[i] * scale;
+        }
+        if (lane == 0)
+        {
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                out[W * a + i] = total[i];
+        }
+    }
+}
+
+void put(std::vector<unsigned char> &blob, const void *p, size_t n)
+{
+    const unsigned char *c = static_cast<const unsigned char *>(p);
+    blob.insert(blob.end(), c, c + n);
+}
+
+// Primary tables as the reference's field integrators lay them out
+// (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
+// cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
+bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa,
+               std::vector<unsigned char> &blob, std::string &err)
+{
+    if (!validArgs(pp) || !validArgs(spa))
+    {
+        err = "pair precision arguments out of range (increments 1..100, blocks >= 1)";
+        return false;
+    }
+    if (!(prim.inner_radius > 0.0) || !(prim.thickness > 0.0) || !(prim.length > 0.0) || !(sec.inner_radius > 0.0) ||
+        !(sec.thickness > 0.0) || !(sec.length > 0.0) || prim.current == 0.0)
+    {
+        err = "coil dimensions must be positive and the primary current non-zero";
+        return false;
+    }
+    const size_t start = blob.size();
+    const bool fast = prim.use_fast_method != 0;
+    const double tBlock = prim.thickness / pp.thickness_blocks, aBlock = kPi / pp.angular_blocks;
+    const double constant = fast ? kMuReduced * prim.current_density * tBlock * aBlock * 2 * 0.25
+                                 : kMuReduced * prim.current_density * (prim.length / pp.length_blocks) * tBlock *
+                                       aBlock * 2 * 0.125;
+    std::vector<double> pt_, pl_, pa_;
+    const double *tx = legendreNodes(pp.thickness_increments), *tw = legendreWeights(pp.thickness_increments);
+    for (int b = 0; b < pp.thickness_blocks; ++b)
+        for (int i = 0; i < pp.thickness_increments; ++i)
+        {
+            pt_.push_back(prim.inner_radius + tBlock * (b + 0.5) + (tBlock * 0.5) * tx[i]);
+            pt_.push_back(constant * tw[i]);
+        }
+    if (!fast)
+    {
+        const double lBlock = prim.length / pp.length_blocks;
+        const double *lx = legendreNodes(pp.length_increments), *lw = legendreWeights(pp.length_increments);
+        for (int b = 0; b < pp.length_blocks; ++b)
+            for (int i = 0; i < pp.length_increments; ++i)
+            {
+                pl_.push_back(-prim.length * 0.5 + lBlock * (b + 0.5) + (lBlock * 0.5) * lx[i]);
+                pl_.push_back(lw[i]);
+            }
+    }
+    const double *ax = legendreNodes(pp.angular_increments), *aw = legendreWeights(pp.angular_increments);
+    for (int b = 0; b < pp.angular_blocks; ++b)
+        for (int i = 0; i < pp.angular_increments; ++i)
+        {
+            pa_.push_back(std::cos(aBlock * (b + 0.5) + (aBlock * 0.5) * ax[i]));
+            pa_.push_back(aw[i]);
+        }
+    // secondary cloud tables
+    std::vector<double> sl_, st_;
+    std::vector<SecAngular> sa_;
+    const double lbs = sec.length / spa.length_blocks, tbs = sec.thickness / spa.thickness_blocks;
+    const double *slx = legendreNodes(spa.length_increments), *slw = legendreWeights(spa.length_increments);
+    for (int b = 0; b < spa.length_blocks; ++b)
+        for (int i = 0; i < spa.length_increments; ++i)
+        {
+            sl_.push_back(-sec.length * 0.5 + lbs * (b + 0.5) + (lbs * 0.5) * slx[i]);
+            sl_.push_back(slw[i]);
+        }
+    const double *stx = legendreNodes(spa.thickness_increments), *stw = legendreWeights(spa.thickness_increments);
+    for (int b = 0; b < spa.thickness_blocks; ++b)
+        for (int i = 0; i < spa.thickness_increments; ++i)
+        {
+            st_.push_back(sec.inner_radius + tbs * (b + 0.5) + (tbs * 0.5) * stx[i]);
+            st_.push_back(stw[i]);
+        }
+    const double *sax = legendreNodes(spa.angular_increments), *saw = legendreWeights(spa.angular_increments);
+    for (int b = 0; b < spa.angular_blocks; ++b)
+        for (int i = 0; i < spa.angular_increments; ++i)
+            sa_.push_back({b + 0.5, sax[i], saw[i], 0.0});
+
+    PairHeader ph;
+    std::memset(&ph, 0, sizeof(ph));
+    SegmentHeader &h = ph.prim;
+    for (int i = 0; i < 3; ++i)
+        h.position[i] = prim.position[i];
+    std::memcpy(h.transform, prim.transform, sizeof(h.transform));
+    std::memcpy(h.inv_transform, prim.inverse_transform, sizeof(h.inv_transform));
+    h.half_length = prim.length * 0.5;
+    h.field_factor = 1.0;
+    h.inner_radius = prim.inner_radius;
+    h.n_t = (int)pt_.size() / 2;
+    h.n_l = (int)pl_.size() / 2;
+    h.n_phi = (int)pa_.size() / 2;
+    h.fast = fast ? 1 : 0;
+    const int hdr16 = (int)sizeof(PairHeader) / 16;
+    h.off_t = hdr16;
+    h.off_l = h.off_t + h.n_t;
+    h.off_phi = h.off_l + h.n_l;
+    ph.s_nl = (int)sl_.size() / 2;
+    ph.s_nt = (int)st_.size() / 2;
+    ph.s_na = (int)sa_.size();
+    ph.s_ablocks = spa.angular_blocks;
+    ph.off_sl = h.off_phi + h.n_phi;
+    ph.off_st = ph.off_sl + ph.s_nl;
+    ph.off_sa = ph.off_st + ph.s_nt;
+    const double blocks = double(spa.length_blocks) * spa.thickness_blocks * spa.angular_blocks;
+    ph.m_factor = 2 * kPi * sec.num_turns / prim.current / blocks;
+    ph.f_factor = 2 * kPi * (sec.current * sec.num_turns) / blocks;
+    ph.prim_y_angle = prim.y_axis_angle;
+    ph.prim_z_angle = prim.z_axis_angle;
+    put(blob, &ph, sizeof(ph));
+    put(blob, pt_.data(), sizeof(double) * pt_.size());
+    put(blob, pl_.data(), sizeof(double) * pl_.size());
+    put(blob, pa_.data(), sizeof(double) * pa_.size());
+    put(blob, sl_.data(), sizeof(double) * sl_.size());
+    put(blob, st_.data(), sizeof(double) * st_.size());
+    put(blob, sa_.data(), sizeof(SecAngular) * sa_.size());
+    (void)start;
+    return true;
+}
+
+struct DevBuf
+{
+    void *p = nullptr;
+    ~DevBuf()
+    {
+        if (p)
+            cudaFree(p);
+    }
+};
+} // namespace
+
+int cudaFail(cudaError_t e, const char *what);
+} // namespace ccoil
+
+using namespace ccoil;
+
+extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                                       const ccoil_precision_args_t *secondary_precisions,
+                                       const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
+                                       long long count, int quantity, int precision, double *out,
+                                       long long *z_axis_count, int memory, void *stream)
+{
+    if (primary_count < 0 || (primary_count > 0 && (!primaries || !secondary_precisions)) || !secondary)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "null coils or negative primary_count");
+    if (count < 0 || (count > 0 && (!secondary_poses || !out)))
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "count < 0 or null poses/out");
+    if (primary_poses && primary_count != 1)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "per-arrangement primary poses need exactly one primary");
+    if (quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE && quantity != CCOIL_PAIR_FORCE_TORQUE)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "quantity must be MUTUAL_INDUCTANCE or FORCE_TORQUE");
+    if (precision != CCOIL_PRECISION_FP64)
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "coil-pair arrangements are evaluated in FP64");
+    if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
+    if (z_axis_count)
+        *z_axis_count = 0;
+    const int width = quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE ? 1 : 6;
+    if (count == 0)
+        return CCOIL_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (primary_count == 0)
+    {
+        cudaError_t e = memory == CCOIL_MEMORY_HOST ? cudaSuccess : cudaMemsetAsync(out, 0, sizeof(double) * width * count, st);
+        if (memory == CCOIL_MEMORY_HOST)
+            std::memset(out, 0, sizeof(double) * width * count);
+        return e == cudaSuccess ? CCOIL_OK : cudaFail(e, "memset");
+    }
+
+    std::vector<unsigned char> blob;
+    std::vector<long long> offsets;
+    std::string err;
+    for (int j = 0; j < primary_count; ++j)
+    {
+        offsets.push_back((long long)blob.size());
+        if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], blob, err))
+            return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
+    }
+    DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ;
+    cudaError_t e = cudaMalloc(&dBlob.p, blob.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dOff.p, sizeof(long long) * offsets.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dZ.p, sizeof(unsigned long long));
+    if (e == cudaSuccess && memory == CCOIL_MEMORY_HOST)
+    {
+        e = cudaMalloc(&dSec.p, sizeof(double) * 5 * count);
+        if (e == cudaSuccess && primary_poses)
+            e = cudaMalloc(&dPrim.p, sizeof(double) * 5 * count);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&dOut.p, sizeof(double) * width * count);
+    }
+    if (e != cudaSuccess)
+        return cudaFail(e, "cudaMalloc");
+    e = cudaMemcpyAsync(dBlob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dOff.p, offsets.data(), sizeof(long long) * offsets.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(dZ.p, 0, sizeof(unsigned long long), st);
+    const double *secP = reinterpret_cast<const double *>(secondary_poses);
+    const double *primP = reinterpret_cast<const double *>(primary_poses);
+    double *o = out;
+    if (e == cudaSuccess && memory == CCOIL_MEMORY_HOST)
+    {
+        e = cudaMemcpyAsync(dSec.p, secondary_poses, sizeof(double) * 5 * count, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && primary_poses)
+            e = cudaMemcpyAsync(dPrim.p, primary_poses, sizeof(double) * 5 * count, cudaMemcpyHostToDevice, st);
+        secP = static_cast<const double *>(dSec.p);
+        primP = primary_poses ? static_cast<const double *>(dPrim.p) : nullptr;
+        o = static_cast<double *>(dOut.p);
+    }
+    if (e != cudaSuccess)
+        return cudaFail(e, "host->device copy");
+    const long long warpsNeeded = count;
+    long long blocks = (warpsNeeded + 3) / 4;
+    if (blocks > 148LL * 64)
+        blocks = 148LL * 64;
+    auto *zc = static_cast<unsigned long long *>(dZ.p);
+    if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
+        pairKernel64<0><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
+                                                           static_cast<const long long *>(dOff.p), primary_count,
+                                                           primP, secP, count, o, zc);
+    else
+        pairKernel64<1><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
+                                                           static_cast<const long long *>(dOff.p), primary_count,
+                                                           primP, secP, count, o, zc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cudaFail(e, "pair kernel launch");
+    if (memory == CCOIL_MEMORY_HOST)
+        e = cudaMemcpyAsync(out, o, sizeof(double) * width * count, cudaMemcpyDeviceToHost, st);
+    unsigned long long zcount = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&zcount, zc, sizeof(zcount), cudaMemcpyDeviceToHost, st);
+    // the temporary device buffers are released on return: wait for the kernel
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return cudaFail(e, "pair arrangements");
+    if (z_axis_count)
+        *z_axis_count = (long long)zcount;
+    return CCOIL_OK;
+}

@@ -163,6 +163,50 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
                              int memory, int lanes_per_point, void *stream);
 int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
 
+/* ------------------------------------------------------------------------ *
+ * Coil pairs over many arrangements                                         *
+ * ------------------------------------------------------------------------ */
+
+typedef enum ccoil_pair_quantity
+{
+    CCOIL_PAIR_MUTUAL_INDUCTANCE = 0, /* M, one double per arrangement */
+    CCOIL_PAIR_FORCE_TORQUE = 1       /* Fx Fy Fz Tx Ty Tz on the secondary, six doubles per arrangement */
+} ccoil_pair_quantity_t;
+
+/* Position and orientation of a coil (Coil::setPositionAndOrientation,
+ * src/Coil/Coil.cxx:245-252). */
+typedef struct ccoil_pose
+{
+    double position[3];
+    double y_axis_angle;
+    double z_axis_angle;
+} ccoil_pose_t;
+
+/* Mutual inductance or force/torque of the secondary with `primary_count`
+ * primaries, for `count` arrangements, with the reference's CPU general-case
+ * algorithm (Coil::calculateMutualInductanceGeneral,
+ * src/Coil/MInductance/CalculateMInductanceGeneral.cxx:8-117, and
+ * Coil::calculateForceTorqueGeneral,
+ * src/Coil/ForceAndTorque/CalculateForceGeneral.cxx:9-131, including the
+ * half-ring rule for coplanar axes).  primaries[j].precision is the primary's
+ * precision for pair j and secondary_precisions[j] the secondary's (as from
+ * ccoil_pair_arguments).  With primary_poses (one per arrangement, exactly one
+ * primary) both coils move: Coil::computeAll{MutualInductance,ForceTorque}Arrangements
+ * (src/Coil/MInductance/ComputeMInductanceMethods.cxx:200-260).  With
+ * primary_poses == NULL the primaries keep their own poses and are summed in
+ * order: CoilGroup::computeAll*Arrangements
+ * (src/CoilGroup/MInductance/ComputeMInductance.cxx:23-64).  Replaces
+ * Calculate_mutual_inductance_configurations[_group] and
+ * Calculate_force_and_torque_configurations[_group]
+ * (src/Coil/CUDAKernels/CoilAcceleration.h:21-29,
+ * src/CoilGroup/CUDAKernels/CoilGroupAcceleration.h:27-37).
+ * Arrangements that are exact z-axis cases (Coil::isZAxisCase) are evaluated
+ * with the general formula; their number is returned in *z_axis_count. */
+int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                            const ccoil_precision_args_t *secondary_precisions, const ccoil_pose_t *primary_poses,
+                            const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
+                            double *out, long long *z_axis_count, int memory, void *stream);
+
 /* Number of device-side wait timeouts seen since the library was loaded (the
  * bounded waits of the staging pipeline; a non-zero value also makes the
  * failing call return CCOIL_ERR_TIMEOUT). */
