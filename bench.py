@@ -37,11 +37,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c", "both"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "fp32c", "both"])
     ap.add_argument("--points", type=int, default=1 << 20)
     ap.add_argument("--coils", type=int, default=128)
     ap.add_argument("--pf", type=float, default=5.0)
-    ap.add_argument("--cpu-sample-points", type=int, default=2048)
+    ap.add_argument("--cpu-sample-points", type=int, default=32768)
+    ap.add_argument("--arrangements", type=int, default=1 << 18,
+                    help="coil-pair arrangements per GPU for the M and F/T part (0 skips it)")
+    ap.add_argument("--cpu-sample-arrangements", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -100,6 +103,59 @@ def reference_arm(a):
                              "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def pair_setup(cc, workloads, n, seed):
+    """The pair workload: RECTANGULAR primary (0.1, 0.05, 0.1, N=200), THIN secondary
+    (0.05, 0, 0.2, N=100), both moving per arrangement; CPU pair arguments at PF 5."""
+    prim_row, sec_row, ppos, spos, py, pz, sy, sz = workloads.pair_config(arrangements=n, seed=seed)
+    prim, sec = workloads.coils_from_rows(prim_row, 5.0)[0], workloads.coils_from_rows(sec_row, 5.0)[0]
+    pp, sp = cc.Coil._pair_args(prim, sec, 5.0)
+    pposes = np.concatenate([ppos, py[:, None], pz[:, None]], axis=1)
+    sposes = np.concatenate([spos, sy[:, None], sz[:, None]], axis=1)
+    return prim_row, sec_row, prim.struct(pp), sec.struct(sp), sp.to_struct(), pposes, sposes, (pp, sp)
+
+
+def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier):
+    import torch
+    from ccoil_b200.coil import pair_arrangements_device
+    _, _, pstruct, sstruct, spre, pposes, sposes, (pp, sp) = pair_setup(cc, workloads, a.arrangements,
+                                                                        3 + 7919 * rank)
+    dp = torch.from_numpy(pposes).to(dev)
+    ds = torch.from_numpy(sposes).to(dev)
+    res = {}
+    for name, q, w in (("M", 0, 1), ("FT", 1, 6)):
+        out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
+        pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out)  # warm-up
+        torch.cuda.synchronize()
+        barrier()
+        ms = 0.0
+        for _ in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            zc = pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms = max_over_ranks(ms / a.steps)
+        res[name] = {"ms": ms, "arrangements_per_s": a.arrangements / (ms * 1e-3), "z_axis_cases": zc}
+    aB, tB, lB, aI, tI, lI = sp.as_tuple()
+    res["secondary_nodes"] = aB * aI * tB * tI * lB * lI
+    res["primary_nodes"] = pp.angular_blocks * pp.angular_increments * pp.thickness_blocks * pp.thickness_increments
+    return res
+
+
+def cpu_arrangement_rate(a, sample):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+    from ccoil_b200 import workloads
+    cores = os.cpu_count() or 1
+    ref = Reference(threads=cores)
+    prim, sec, ppos, spos, py, pz, sy, sz = workloads.pair_config(arrangements=sample, seed=3)
+    t0 = time.perf_counter()
+    ref.m_arrangements(prim, sec, ppos, spos, py, pz, sy, sz, pf=5.0, method=1)
+    dt = time.perf_counter() - t0
+    return sample / dt, cores, dt
 
 
 # ---------------------------------------------------------------------------
@@ -295,10 +351,28 @@ def main():
             e = (results[1]["outs"][name] - r64["outs"][name]).norm(dim=1) / r64["outs"][name].norm(dim=1)
             errs[name] = {"max": float(e.max()), "median": float(e.median())}
         line["fp32c_rel_err_vs_fp64"] = errs
+    if a.arrangements > 0:
+        arr = bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier)
+        line["arrangements"] = {"workload": "RECTANGULAR primary (0.1, 0.05, 0.1 m, N=200) x THIN secondary "
+                                            "(0.05, 0, 0.2 m, N=100), %d arrangements per GPU, offsets in a "
+                                            "0.6 m cube, random orientations, 5%% near-coaxial, PF 5, FP64"
+                                            % a.arrangements,
+                                "M_arrangements_per_s": arr["M"]["arrangements_per_s"] * world,
+                                "FT_arrangements_per_s": arr["FT"]["arrangements_per_s"] * world,
+                                "M_ms": arr["M"]["ms"], "FT_ms": arr["FT"]["ms"],
+                                "secondary_nodes": arr["secondary_nodes"], "primary_nodes": arr["primary_nodes"],
+                                "z_axis_cases": arr["M"]["z_axis_cases"]}
+        line["gpu_launches"] += 2 * a.steps
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, cores, dt, desc = cpu_reference_rate(a, a.cpu_sample_points)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
                                 "sample": desc, "seconds": dt}
+        if a.arrangements > 0 and a.cpu_sample_arrangements > 0:
+            arate, acores, adt = cpu_arrangement_rate(a, a.cpu_sample_arrangements)
+            line["cpu_baseline"]["M_arrangements_per_s"] = arate
+            line["cpu_baseline"]["arrangement_sample"] = ("%d arrangements of the pair workload, "
+                                                          "Coil::computeAllMutualInductanceArrangements CPU_MT"
+                                                          % a.cpu_sample_arrangements)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -220,6 +220,25 @@ def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, seco
     return (out[:, 0] if width == 1 else out), zc.value
 
 
+def pair_arrangements_device(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity,
+                             out, stream=None):
+    """Device-memory variant: poses (n, 5) and out are torch CUDA float64 tensors
+    (primary_poses may be None for fixed primaries); asynchronous on `stream`
+    up to the library's own completion wait."""
+    import torch
+    n = secondary_poses.shape[0]
+    prim = (_lib.CoilStruct * max(len(primaries), 1))(*primaries)
+    secp = (_lib.PrecisionArgsStruct * max(len(sec_precisions), 1))(*sec_precisions)
+    zc = ctypes.c_longlong(0)
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(lib().ccoil_pair_arrangements(
+        prim, len(primaries), ctypes.byref(secondary), secp,
+        None if primary_poses is None else ctypes.c_void_p(primary_poses.data_ptr()),
+        ctypes.c_void_p(secondary_poses.data_ptr()), n, quantity, _lib.PRECISION_FP64,
+        ctypes.c_void_p(out.data_ptr()), ctypes.byref(zc), _lib.MEMORY_DEVICE, ctypes.c_void_p(st)))
+    return zc.value
+
+
 _next_id = [0]
 
 
