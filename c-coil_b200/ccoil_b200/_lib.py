@@ -84,6 +84,12 @@ def lib():
     L.ccoil_field_plan_execute.argtypes = [vp, vp, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_int, vp]
     L.ccoil_field_plan_destroy.argtypes = [vp]
     L.ccoil_timeout_count.restype = ctypes.c_longlong
+    L.ccoil_batch_plan_create.argtypes = [cp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ccoil_batch_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.ccoil_batch_plan_tune.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
+    L.ccoil_batch_plan_set_split.argtypes = [vp, ctypes.c_int]
+    L.ccoil_batch_plan_destroy.argtypes = [vp]
     L.ccoil_pair_arrangements.argtypes = [cp, ctypes.c_int, cp, pp, vp, vp, ctypes.c_longlong, ctypes.c_int,
                                           ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, vp]
     _lib = L

@@ -114,6 +114,26 @@ struct FieldLaunch
 constexpr size_t kNearPairBytes = 8;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
+
+// batched persistent launch (fields.cu, batch.cuh)
+struct BatchLaunch
+{
+    const unsigned char *d_blob;
+    const SegmentDesc *d_segs;
+    const void *d_items;  // BatchItem[nitems]
+    int nitems;
+    unsigned *d_next;     // item counter (scratch)
+    const double *d_points;
+    double *d_outA, *d_outB, *d_outG;
+    int precision;
+    int grid;
+    void *d_work = nullptr;
+    unsigned long long work_capacity = 0;
+    unsigned long long *d_work_count = nullptr;
+};
+constexpr size_t kBatchItemBytes = 32;
+int launchBatch(const BatchLaunch &B, void *stream);
+int batchBlocksPerSM(int precision);
 } // namespace ccoil
 
 #endif

@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
 }
 
 #include "fields32.cuh"
+#include "batch.cuh"
 
 template <int FIELD>
 cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
@@ -242,6 +243,23 @@ int launchFields(const FieldLaunch &L, void *stream)
     if (e != cudaSuccess)
         return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     return CCOIL_OK;
+}
+
+int launchBatch(const BatchLaunch &B, void *stream)
+{
+    static_assert(sizeof(BatchItem) == kBatchItemBytes, "batch item layout");
+    return launchBatchImpl(B, static_cast<cudaStream_t>(stream));
+}
+
+int batchBlocksPerSM(int precision)
+{
+    int n = 0;
+    const size_t smem = (size_t)kSegmentStages * kSegmentBytes;
+    cudaError_t e = precision == CCOIL_PRECISION_FP64
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<CCOIL_PRECISION_FP64>, 128, smem)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &n, batchKernel<CCOIL_PRECISION_FP32_COMPENSATED>, 128, smem);
+    return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 int readTimeouts(long long &count)

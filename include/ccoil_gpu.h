@@ -207,6 +207,35 @@ int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, co
                             const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
                             double *out, long long *z_axis_count, int memory, void *stream);
 
+/* ------------------------------------------------------------------------ *
+ * Batched independent systems                                               *
+ * ------------------------------------------------------------------------ */
+
+/* Many independent coil systems (each what the reference evaluates with one
+ * CoilGroup::computeAll*(points, GPU), src/CoilGroup/Fields/CalculateFieldsGPU.cxx:11-196)
+ * evaluated by one persistent launch, replayed from a captured CUDA graph.
+ * System s owns coils [system_coil_offsets[s], system_coil_offsets[s+1]) and
+ * points [system_point_offsets[s], system_point_offsets[s+1]) of the flat
+ * arrays; fields_mask combines 1<<CCOIL_FIELD_A, 1<<CCOIL_FIELD_B and
+ * 1<<CCOIL_FIELD_G; every requested field is computed in the same launch. */
+typedef struct ccoil_batch_plan ccoil_batch_plan_t;
+
+int ccoil_batch_plan_create(const ccoil_coil_t *coils, const int *system_coil_offsets,
+                            const long long *system_point_offsets, int system_count, int fields_mask, int precision,
+                            ccoil_batch_plan_t **plan);
+/* points, out_a/out_b/out_g: device pointers (outputs of unrequested fields may
+ * be NULL); the first call with a given set of pointers captures the graph,
+ * later calls replay it; ordered after and before `stream`. */
+int ccoil_batch_plan_execute(ccoil_batch_plan_t *plan, const double *points, double *out_a, double *out_b,
+                             double *out_g, void *stream);
+/* Autotuner: times the batch with each candidate item split (the minimum number
+ * of work items per system and field before more lanes per point stop being
+ * added) and keeps the fastest; reports it and its time. */
+int ccoil_batch_plan_tune(ccoil_batch_plan_t *plan, const double *points, double *out_a, double *out_b,
+                          double *out_g, int *chosen_split, float *best_ms);
+int ccoil_batch_plan_set_split(ccoil_batch_plan_t *plan, int split);
+int ccoil_batch_plan_destroy(ccoil_batch_plan_t *plan);
+
 /* Number of device-side wait timeouts seen since the library was loaded (the
  * bounded waits of the staging pipeline; a non-zero value also makes the
  * failing call return CCOIL_ERR_TIMEOUT). */
