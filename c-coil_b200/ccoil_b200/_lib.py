@@ -46,7 +46,7 @@ class PoseStruct(ctypes.Structure):
                 ("z_axis_angle", ctypes.c_double)]
 
 
-PAIR_MUTUAL_INDUCTANCE, PAIR_FORCE_TORQUE = 0, 1
+PAIR_MUTUAL_INDUCTANCE, PAIR_FORCE_TORQUE, PAIR_MUTUAL_INDUCTANCE_GRADIENT = 0, 1, 2
 
 
 class CCoilError(RuntimeError):
@@ -90,6 +90,7 @@ def lib():
     L.ccoil_batch_plan_tune.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
     L.ccoil_batch_plan_set_split.argtypes = [vp, ctypes.c_int]
     L.ccoil_batch_plan_destroy.argtypes = [vp]
+    L.ccoil_b_field_adjoint.argtypes = [dp, pp, ctypes.c_int, vp, ctypes.c_longlong, vp, vp, vp]
     L.ccoil_pair_arrangements.argtypes = [cp, ctypes.c_int, cp, pp, vp, vp, ctypes.c_longlong, ctypes.c_int,
                                           ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, vp]
     _lib = L

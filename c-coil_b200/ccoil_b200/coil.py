@@ -207,7 +207,8 @@ def _poses(positions, y_angles, z_angles):
 def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity):
     """Runs ccoil_pair_arrangements; returns (values, number of exact z-axis arrangements)."""
     n = len(secondary_poses)
-    width = 1 if quantity == _lib.PAIR_MUTUAL_INDUCTANCE else 6
+    width = {_lib.PAIR_MUTUAL_INDUCTANCE: 1, _lib.PAIR_FORCE_TORQUE: 6,
+             _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT: 3}[quantity]
     out = np.zeros((n, width))
     prim = (_lib.CoilStruct * max(len(primaries), 1))(*primaries)
     secp = (_lib.PrecisionArgsStruct * max(len(sec_precisions), 1))(*sec_precisions)
@@ -368,6 +369,18 @@ class Coil:
                                   primary_z_angles, secondary_y_angles, secondary_z_angles,
                                   precision_factor or PrecisionFactor(), compute_method,
                                   _lib.PAIR_MUTUAL_INDUCTANCE)
+
+    @staticmethod
+    def compute_all_mutual_inductance_gradient_arrangements(primary, secondary, primary_positions,
+                                                            secondary_positions, primary_y_angles, primary_z_angles,
+                                                            secondary_y_angles, secondary_z_angles,
+                                                            precision_factor=None, compute_method=ComputeMethod.GPU):
+        """dM/d(secondary position) per arrangement, (n, 3): the exact derivative of the mutual
+        inductance quadrature (no counterpart in the reference)."""
+        return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
+                                  primary_z_angles, secondary_y_angles, secondary_z_angles,
+                                  precision_factor or PrecisionFactor(), compute_method,
+                                  _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT)
 
     @staticmethod
     def compute_all_force_torque_arrangements(primary, secondary, primary_positions, secondary_positions,

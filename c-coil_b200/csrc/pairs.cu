@@ -127,6 +127,64 @@ __device__ __forceinline__ Frame frameAt(const Pose &P, const double *q)
     return toCoilFrame(h, q[0], q[1], q[2]);
 }
 
+// A_phi of the primary at a point and its derivatives in r and z (coil frame):
+//   fast node  a = r' c [asinh(top/rho) - asinh(bot/rho)],
+//              da/dz = r' c (g1 - g2),  da/dr = -r' c (r - r' c)(top g1 - bot g2) / rho^2
+//   slow node  a = r' c / sqrt(D),  da/dz = -r' c zl D^-3/2,  da/dr = -r' c (r - r' c) D^-3/2
+// (the value `a` uses the reference's operation sequence, as segmentA64)
+__device__ __forceinline__ void segmentAGrad64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                               const double2 *pt, const Frame &f, double &A, double &Ar, double &Az)
+{
+    A = segmentA64<1>(h, tt, lt, pt, f, 0);
+    Ar = 0.0;
+    Az = 0.0;
+    const double r = f.r;
+    if (h.fast)
+    {
+        const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            double sr = 0.0, sz = 0.0;
+            for (int k = 0; k < h.n_phi; ++k)
+            {
+                const double2 q = pt[k];
+                const double c = q.x;
+                const double rho2 = t.x * t.x + r * r - 2.0 * t.x * r * c;
+                const double g1 = rsqrt(rho2 + top * top), g2 = rsqrt(rho2 + bot * bot);
+                sz += q.y * c * (g1 - g2);
+                sr -= q.y * c * (r - t.x * c) * (top * g1 - bot * g2) / rho2;
+            }
+            Ar += t.y * t.x * sr;
+            Az += t.y * t.x * sz;
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            const double2 l = lt[i];
+            const double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                double sr = 0.0, sz = 0.0;
+                for (int k = 0; k < h.n_phi; ++k)
+                {
+                    const double2 q = pt[k];
+                    const double c = q.x;
+                    const double D = t.x * t.x + r * r - 2.0 * t.x * r * c + zl * zl;
+                    const double g = rsqrt(D), g3 = g * g * g;
+                    sz -= q.y * c * zl * g3;
+                    sr -= q.y * c * (r - t.x * c) * g3;
+                }
+                Ar += l.y * t.y * t.x * sr;
+                Az += l.y * t.y * t.x * sz;
+            }
+        }
+    }
+}
+
 template <int QTY>
 __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restrict__ blob,
                                                     const long long *__restrict__ primOffsets, int nprim,
@@ -135,7 +193,7 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
                                                     double *__restrict__ out,
                                                     unsigned long long *__restrict__ zAxisCount)
 {
-    constexpr int W = QTY == 0 ? 1 : 6;
+    constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : 3;
     const int lane = threadIdx.x % 32;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const long long warps = (long long)gridDim.x * blockDim.x / 32;
@@ -184,7 +242,7 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
             if (lane == 0 && zAxisCount && zAxisCase(ppose, sp, h.inner_radius))
                 atomicAdd(zAxisCount, 1ull);
             double offset = 0.0;
-            const bool improved = QTY == 0 ? improvedCase(ppose, sp, offset) : false;
+            const bool improved = QTY != 1 ? improvedCase(ppose, sp, offset) : false;
             const double ablk = (improved ? kPi : 2 * kPi) / ph.s_ablocks;
             const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
             double part[W];
@@ -214,6 +272,28 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
                                  Az = P.T[6] * vx + P.T[7] * vy;
                     part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
                 }
+                else if (QTY == 2)
+                {
+                    // dM/d(secondary position) = factor sum_n w_n J_A(q_n)^T t_n,
+                    // J_A = T J_loc T^T; J_loc of A_loc = a(r, z) (-sin, cos, 0)
+                    double av, ar, az;
+                    segmentAGrad64(h, tt, lt, pt, f, av, ar, az);
+                    const double c = f.cphi, s_ = f.sphi;
+                    const double ao = f.r > 0.0 ? av / f.r : ar;
+                    const double J[9] = {s_ * c * (ao - ar), -s_ * s_ * ar - c * c * ao, -s_ * az,
+                                         c * c * ar + s_ * s_ * ao, s_ * c * (ar - ao), c * az,
+                                         0.0, 0.0, 0.0};
+                    // T J^T T^T t
+                    double u[3], v[3], o[3];
+                    for (int i = 0; i < 3; ++i)
+                        u[i] = P.T[i] * tan[0] + P.T[3 + i] * tan[1] + P.T[6 + i] * tan[2];  // T^T t
+                    for (int i = 0; i < 3; ++i)
+                        v[i] = J[i] * u[0] + J[3 + i] * u[1] + J[6 + i] * u[2];           // J^T u
+                    for (int i = 0; i < 3; ++i)
+                        o[i] = P.T[3 * i] * v[0] + P.T[3 * i + 1] * v[1] + P.T[3 * i + 2] * v[2];
+                    for (int i = 0; i < 3; ++i)
+                        part[i] += o[i] * w;
+                }
                 else
                 {
                     double H, Z;
@@ -239,7 +319,7 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
 #pragma unroll
                 for (int i = 0; i < W; ++i)
                     part[i] += __shfl_xor_sync(0xffffffffu, part[i], off);
-            const double scale = QTY == 0 ? ph.m_factor : ph.f_factor;
+            const double scale = QTY == 1 ? ph.f_factor : ph.m_factor;
 #pragma unroll
             for (int i = 0; i < W; ++i)
                 total[i] += part[i] * scale;
@@ -400,15 +480,16 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "count < 0 or null poses/out");
     if (primary_poses && primary_count != 1)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "per-arrangement primary poses need exactly one primary");
-    if (quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE && quantity != CCOIL_PAIR_FORCE_TORQUE)
-        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "quantity must be MUTUAL_INDUCTANCE or FORCE_TORQUE");
+    if (quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE && quantity != CCOIL_PAIR_FORCE_TORQUE &&
+        quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown pair quantity");
     if (precision != CCOIL_PRECISION_FP64)
         return failMessage(CCOIL_ERR_NOT_SUPPORTED, "coil-pair arrangements are evaluated in FP64");
     if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
     if (z_axis_count)
         *z_axis_count = 0;
-    const int width = quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE ? 1 : 6;
+    const int width = quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE ? 1 : quantity == CCOIL_PAIR_FORCE_TORQUE ? 6 : 3;
     if (count == 0)
         return CCOIL_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -473,8 +554,12 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
         pairKernel64<0><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
                                                            static_cast<const long long *>(dOff.p), primary_count,
                                                            primP, secP, count, o, zc);
-    else
+    else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
         pairKernel64<1><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
+                                                           static_cast<const long long *>(dOff.p), primary_count,
+                                                           primP, secP, count, o, zc);
+    else
+        pairKernel64<2><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
                                                            static_cast<const long long *>(dOff.p), primary_count,
                                                            primP, secP, count, o, zc);
     e = cudaGetLastError();

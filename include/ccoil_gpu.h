@@ -170,7 +170,10 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
 typedef enum ccoil_pair_quantity
 {
     CCOIL_PAIR_MUTUAL_INDUCTANCE = 0, /* M, one double per arrangement */
-    CCOIL_PAIR_FORCE_TORQUE = 1       /* Fx Fy Fz Tx Ty Tz on the secondary, six doubles per arrangement */
+    CCOIL_PAIR_FORCE_TORQUE = 1,      /* Fx Fy Fz Tx Ty Tz on the secondary, six doubles per arrangement */
+    CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT = 2 /* dM/d(secondary position): the exact derivative of the M
+                                                 quadrature (adjoint of M; no counterpart in the reference),
+                                                 three doubles per arrangement */
 } ccoil_pair_quantity_t;
 
 /* Position and orientation of a coil (Coil::setPositionAndOrientation,
@@ -235,6 +238,21 @@ int ccoil_batch_plan_tune(ccoil_batch_plan_t *plan, const double *points, double
                           double *out_g, int *chosen_split, float *best_ms);
 int ccoil_batch_plan_set_split(ccoil_batch_plan_t *plan, int split);
 int ccoil_batch_plan_destroy(ccoil_batch_plan_t *plan);
+
+/* ------------------------------------------------------------------------ *
+ * Adjoint                                                                   *
+ * ------------------------------------------------------------------------ */
+
+/* Gradient of a loss L(B) with respect to each coil's parameters, given
+ * grad_b = dL/dB at the points (no counterpart in the reference, which has no
+ * derivatives).  params: coil_count x 9 host doubles
+ * {R, a, b, N*I, x, y, z, yAxisAngle, zAxisAngle} with the fixed precision
+ * arguments `precisions` (host); points, grad_b (point_count x 3) and
+ * grad_params (coil_count x 9) are device pointers.  Fast-method coils only
+ * (RECTANGULAR, THIN); FP64; deterministic. */
+int ccoil_b_field_adjoint(const double *params, const ccoil_precision_args_t *precisions, int coil_count,
+                          const double *points, long long point_count, const double *grad_b, double *grad_params,
+                          void *stream);
 
 /* Number of device-side wait timeouts seen since the library was loaded (the
  * bounded waits of the staging pipeline; a non-zero value also makes the
