@@ -18,10 +18,11 @@ struct Frame
 // no fused multiply-add), then (z, sqrt(x^2 + y^2), atan2(y, x)) as
 // Vector3::getAsCylindricalCoords (Vector3.cxx:99-102); cos and sin of the
 // azimuth are taken as x/r and y/r
-__device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, double py, double pz)
+// (T is double, or volatile double for a pose kept in shared memory)
+template <typename T>
+__device__ __forceinline__ Frame toCoilFrameAt(const T *pos, const T *M, double px, double py, double pz)
 {
-    const double *M = h.inv_transform;
-    double dx = __dsub_rn(px, h.position[0]), dy = __dsub_rn(py, h.position[1]), dz = __dsub_rn(pz, h.position[2]);
+    double dx = __dsub_rn(px, pos[0]), dy = __dsub_rn(py, pos[1]), dz = __dsub_rn(pz, pos[2]);
     double x = __dadd_rn(__dadd_rn(__dmul_rn(M[0], dx), __dmul_rn(M[1], dy)), __dmul_rn(M[2], dz));
     double y = __dadd_rn(__dadd_rn(__dmul_rn(M[3], dx), __dmul_rn(M[4], dy)), __dmul_rn(M[5], dz));
     Frame f;
@@ -38,6 +39,11 @@ __device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, 
         f.sphi = 0.0;
     }
     return f;
+}
+
+__device__ __forceinline__ Frame toCoilFrame(const SegmentHeader &h, double px, double py, double pz)
+{
+    return toCoilFrameAt(h.position, h.inv_transform, px, py, pz);
 }
 
 // ---------------------------------------------------------------------------

@@ -117,16 +117,6 @@ __device__ __forceinline__ bool zAxisCase(const double *pp, const double *sp, do
            fabs(sp[1] / primR) < 1e-12 && fabs(pp[3] / (2 * kPi)) < 1e-12 && fabs(sp[3] / (2 * kPi)) < 1e-12;
 }
 
-__device__ __forceinline__ Frame frameAt(const Pose &P, const double *q)
-{
-    SegmentHeader h;  // only position / inverse transform are read
-    for (int i = 0; i < 3; ++i)
-        h.position[i] = P.pos[i];
-    for (int i = 0; i < 9; ++i)
-        h.inv_transform[i] = P.Ti[i];
-    return toCoilFrame(h, q[0], q[1], q[2]);
-}
-
 // A_phi of the primary at a point and its derivatives in r and z (coil frame):
 //   fast node  a = r' c [asinh(top/rho) - asinh(bot/rho)],
 //              da/dz = r' c (g1 - g2),  da/dr = -r' c (r - r' c)(top g1 - bot g2) / rho^2
@@ -185,31 +175,58 @@ __device__ __forceinline__ void segmentAGrad64(const SegmentHeader &h, const dou
     }
 }
 
-template <int QTY>
-__global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restrict__ blob,
-                                                    const long long *__restrict__ primOffsets, int nprim,
-                                                    const double *__restrict__ primPoses,
-                                                    const double *__restrict__ secPoses, long long count,
-                                                    double *__restrict__ out,
-                                                    unsigned long long *__restrict__ zAxisCount)
+#ifndef CCOIL_PAIR_MIN_BLOCKS
+#define CCOIL_PAIR_MIN_BLOCKS 6
+#endif
+// largest single-primary blob staged in shared memory (0 turns staging off)
+#ifndef CCOIL_PAIR_STAGE_MAX_BYTES
+#define CCOIL_PAIR_STAGE_MAX_BYTES (48 * 1024)
+#endif
+
+// What a warp needs of its current arrangement and primary, written by lane 0
+// into shared memory and read back by all lanes inside the secondary-node loop
+// (volatile: kept out of registers, which the primary quadrature needs)
+struct WarpPose
 {
+    double pos[3], T[9], Ti[9];  // primary pose
+    double sp[3];                // secondary centre
+    double sA, cA, sB, cB;       // sin / cos of the secondary's y and z axis angles
+    double offset, ablk;         // secondary azimuth offset and angular block size
+};
+
+// stagedBytes > 0: there is one primary and its whole pair blob (stagedBytes,
+// a multiple of 16) is copied into shared memory once per CTA, so the inner
+// quadrature reads its tables from shared memory instead of through L1
+template <int QTY>
+__global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
+    pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
+                 const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
+                 double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes)
+{
+    extern __shared__ __align__(16) unsigned char stagedPair[];
+    __shared__ WarpPose warpPoses[4];
+    if (stagedBytes > 0)
+    {
+        const int4 *src = reinterpret_cast<const int4 *>(blob + primOffsets[0]);
+        int4 *dst = reinterpret_cast<int4 *>(stagedPair);
+        for (int i = threadIdx.x; i < stagedBytes / 16; i += blockDim.x)
+            dst[i] = src[i];
+        __syncthreads();
+    }
     constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : 3;
     const int lane = threadIdx.x % 32;
+    volatile WarpPose &S = warpPoses[threadIdx.x / 32];
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const long long warps = (long long)gridDim.x * blockDim.x / 32;
     for (long long a = warp; a < count; a += warps)
     {
-        const double *sp = secPoses + 5 * a;
-        double sA, cA, sB, cB;
-        sincos(sp[3], &sA, &cA);
-        sincos(sp[4], &sB, &cB);
         double total[W];
 #pragma unroll
         for (int i = 0; i < W; ++i)
             total[i] = 0.0;
         for (int j = 0; j < nprim; ++j)
         {
-            const unsigned char *base = blob + primOffsets[j];
+            const unsigned char *base = stagedBytes > 0 ? stagedPair : blob + primOffsets[j];
             const PairHeader &ph = *reinterpret_cast<const PairHeader *>(base);
             const SegmentHeader &h = ph.prim;
             const double2 *tt = reinterpret_cast<const double2 *>(base) + h.off_t;
@@ -219,31 +236,57 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
             const double2 *st = reinterpret_cast<const double2 *>(base) + ph.off_st;
             const SecAngular *sa = reinterpret_cast<const SecAngular *>(reinterpret_cast<const double2 *>(base) +
                                                                         ph.off_sa);
-            Pose P;
-            double ppose[5];
-            if (primPoses)
+            __syncwarp();  // every lane is done with the previous pose
+            if (lane == 0)
             {
+                const double *sp = secPoses + 5 * a;
+                Pose P;
+                double ppose[5], spose[5];
                 for (int i = 0; i < 5; ++i)
-                    ppose[i] = primPoses[5 * a + i];
-                poseFromAngles(ppose, P);
-            }
-            else
-            {
+                    spose[i] = sp[i];
+                if (primPoses)
+                {
+                    for (int i = 0; i < 5; ++i)
+                        ppose[i] = primPoses[5 * a + i];
+                    poseFromAngles(ppose, P);
+                }
+                else
+                {
+                    for (int i = 0; i < 3; ++i)
+                        P.pos[i] = ppose[i] = h.position[i];
+                    for (int i = 0; i < 9; ++i)
+                    {
+                        P.T[i] = h.transform[i];
+                        P.Ti[i] = h.inv_transform[i];
+                    }
+                    ppose[3] = ph.prim_y_angle;
+                    ppose[4] = ph.prim_z_angle;
+                }
+                if (zAxisCount && zAxisCase(ppose, spose, h.inner_radius))
+                    atomicAdd(zAxisCount, 1ull);
+                double offset = 0.0;
+                const bool improved = QTY != 1 ? improvedCase(ppose, spose, offset) : false;
                 for (int i = 0; i < 3; ++i)
-                    P.pos[i] = ppose[i] = h.position[i];
+                {
+                    S.pos[i] = P.pos[i];
+                    S.sp[i] = spose[i];
+                }
                 for (int i = 0; i < 9; ++i)
                 {
-                    P.T[i] = h.transform[i];
-                    P.Ti[i] = h.inv_transform[i];
+                    S.T[i] = P.T[i];
+                    S.Ti[i] = P.Ti[i];
                 }
-                ppose[3] = ph.prim_y_angle;
-                ppose[4] = ph.prim_z_angle;
+                double sA, cA, sB, cB;
+                sincos(spose[3], &sA, &cA);
+                sincos(spose[4], &sB, &cB);
+                S.sA = sA;
+                S.cA = cA;
+                S.sB = sB;
+                S.cB = cB;
+                S.offset = offset;
+                S.ablk = (improved ? kPi : 2 * kPi) / ph.s_ablocks;
             }
-            if (lane == 0 && zAxisCount && zAxisCase(ppose, sp, h.inner_radius))
-                atomicAdd(zAxisCount, 1ull);
-            double offset = 0.0;
-            const bool improved = QTY != 1 ? improvedCase(ppose, sp, offset) : false;
-            const double ablk = (improved ? kPi : 2 * kPi) / ph.s_ablocks;
+            __syncwarp();
             const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
             double part[W];
 #pragma unroll
@@ -255,21 +298,23 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
                 const int t = lt_i % ph.s_nt, l = lt_i / ph.s_nt;
                 const double2 L = sl[l], R = st[t];
                 const SecAngular A = sa[k];
-                const double phi = (offset + ablk * A.bpos) + (ablk * 0.5) * A.x;
+                const double ablk = S.ablk;
+                const double phi = (S.offset + ablk * A.bpos) + (ablk * 0.5) * A.x;
                 double sP, cP;
                 sincos(phi, &sP, &cP);
+                const double sA = S.sA, cA = S.cA, sB = S.sB, cB = S.cB;
                 const double ringP[3] = {cB * cA * cP - sB * sP, sB * cA * cP + cB * sP, -sA * cP};
                 const double tan[3] = {-cB * cA * sP - sB * cP, -sB * cA * sP + cB * cP, sA * sP};
-                const double q[3] = {sp[0] + L.x * sA * cB + R.x * ringP[0], sp[1] + L.x * sA * sB + R.x * ringP[1],
-                                     sp[2] + L.x * cA + R.x * ringP[2]};
+                const double q[3] = {S.sp[0] + L.x * sA * cB + R.x * ringP[0],
+                                     S.sp[1] + L.x * sA * sB + R.x * ringP[1], S.sp[2] + L.x * cA + R.x * ringP[2]};
                 const double w = 0.125 * R.x * L.y * R.y * A.w;
-                const Frame f = frameAt(P, q);
+                const Frame f = toCoilFrameAt(S.pos, S.Ti, q[0], q[1], q[2]);
                 if (QTY == 0)
                 {
                     const double av = segmentA64<1>(h, tt, lt, pt, f, 0);
                     const double vx = -av * f.sphi, vy = av * f.cphi;
-                    const double Ax = P.T[0] * vx + P.T[1] * vy, Ay = P.T[3] * vx + P.T[4] * vy,
-                                 Az = P.T[6] * vx + P.T[7] * vy;
+                    const double Ax = S.T[0] * vx + S.T[1] * vy, Ay = S.T[3] * vx + S.T[4] * vy,
+                                 Az = S.T[6] * vx + S.T[7] * vy;
                     part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
                 }
                 else if (QTY == 2)
@@ -286,11 +331,11 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
                     // T J^T T^T t
                     double u[3], v[3], o[3];
                     for (int i = 0; i < 3; ++i)
-                        u[i] = P.T[i] * tan[0] + P.T[3 + i] * tan[1] + P.T[6 + i] * tan[2];  // T^T t
+                        u[i] = S.T[i] * tan[0] + S.T[3 + i] * tan[1] + S.T[6 + i] * tan[2];  // T^T t
                     for (int i = 0; i < 3; ++i)
                         v[i] = J[i] * u[0] + J[3 + i] * u[1] + J[6 + i] * u[2];           // J^T u
                     for (int i = 0; i < 3; ++i)
-                        o[i] = P.T[3 * i] * v[0] + P.T[3 * i + 1] * v[1] + P.T[3 * i + 2] * v[2];
+                        o[i] = S.T[3 * i] * v[0] + S.T[3 * i + 1] * v[1] + S.T[3 * i + 2] * v[2];
                     for (int i = 0; i < 3; ++i)
                         part[i] += o[i] * w;
                 }
@@ -299,13 +344,13 @@ __global__ void __launch_bounds__(128) pairKernel64(const unsigned char *__restr
                     double H, Z;
                     segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
                     const double vx = H * f.cphi, vy = H * f.sphi;
-                    const double B[3] = {P.T[0] * vx + P.T[1] * vy + P.T[2] * Z, P.T[3] * vx + P.T[4] * vy + P.T[5] * Z,
-                                         P.T[6] * vx + P.T[7] * vy + P.T[8] * Z};
+                    const double B[3] = {S.T[0] * vx + S.T[1] * vy + S.T[2] * Z, S.T[3] * vx + S.T[4] * vy + S.T[5] * Z,
+                                         S.T[6] * vx + S.T[7] * vy + S.T[8] * Z};
                     double dF[3], dT[3];
                     cross3(tan, B, dF);
                     for (int i = 0; i < 3; ++i)
                         dF[i] *= w;
-                    const double rel[3] = {q[0] - sp[0], q[1] - sp[1], q[2] - sp[2]};
+                    const double rel[3] = {q[0] - S.sp[0], q[1] - S.sp[1], q[2] - S.sp[2]};
                     cross3(rel, dF, dT);
                     for (int i = 0; i < 3; ++i)
                     {
@@ -545,23 +590,25 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     }
     if (e != cudaSuccess)
         return cudaFail(e, "host->device copy");
+    // one primary whose tables fit: stage them in shared memory
+    const int stagedBytes = (primary_count == 1 && blob.size() <= CCOIL_PAIR_STAGE_MAX_BYTES && blob.size() % 16 == 0) ? (int)blob.size() : 0;
     const long long warpsNeeded = count;
     long long blocks = (warpsNeeded + 3) / 4;
     if (blocks > 148LL * 64)
         blocks = 148LL * 64;
     auto *zc = static_cast<unsigned long long *>(dZ.p);
     if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
-        pairKernel64<0><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
-                                                           static_cast<const long long *>(dOff.p), primary_count,
-                                                           primP, secP, count, o, zc);
+        pairKernel64<0><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
+            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
+            secP, count, o, zc, stagedBytes);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
-        pairKernel64<1><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
-                                                           static_cast<const long long *>(dOff.p), primary_count,
-                                                           primP, secP, count, o, zc);
+        pairKernel64<1><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
+            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
+            secP, count, o, zc, stagedBytes);
     else
-        pairKernel64<2><<<(unsigned)blocks, 128, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
-                                                           static_cast<const long long *>(dOff.p), primary_count,
-                                                           primP, secP, count, o, zc);
+        pairKernel64<2><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
+            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
+            secP, count, o, zc, stagedBytes);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return cudaFail(e, "pair kernel launch");
