@@ -204,7 +204,8 @@ def _poses(positions, y_angles, z_angles):
     return np.ascontiguousarray(np.concatenate([pos, y[:, None], z[:, None]], axis=1))
 
 
-def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity):
+def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity,
+                       precision_mode=PrecisionMode.FP64):
     """Runs ccoil_pair_arrangements; returns (values, number of exact z-axis arrangements)."""
     n = len(secondary_poses)
     width = {_lib.PAIR_MUTUAL_INDUCTANCE: 1, _lib.PAIR_FORCE_TORQUE: 6,
@@ -216,13 +217,13 @@ def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, seco
     check(lib().ccoil_pair_arrangements(
         prim, len(primaries), ctypes.byref(secondary), secp,
         None if primary_poses is None else primary_poses.ctypes.data_as(ctypes.c_void_p),
-        secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, _lib.PRECISION_FP64,
+        secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, int(precision_mode),
         out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(zc), _lib.MEMORY_HOST, None))
     return (out[:, 0] if width == 1 else out), zc.value
 
 
 def pair_arrangements_device(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity,
-                             out, stream=None):
+                             out, stream=None, precision_mode=PrecisionMode.FP64):
     """Device-memory variant: poses (n, 5) and out are torch CUDA float64 tensors
     (primary_poses may be None for fixed primaries); asynchronous on `stream`
     up to the library's own completion wait."""
@@ -235,7 +236,7 @@ def pair_arrangements_device(primaries, secondary, sec_precisions, primary_poses
     check(lib().ccoil_pair_arrangements(
         prim, len(primaries), ctypes.byref(secondary), secp,
         None if primary_poses is None else ctypes.c_void_p(primary_poses.data_ptr()),
-        ctypes.c_void_p(secondary_poses.data_ptr()), n, quantity, _lib.PRECISION_FP64,
+        ctypes.c_void_p(secondary_poses.data_ptr()), n, quantity, int(precision_mode),
         ctypes.c_void_p(out.data_ptr()), ctypes.byref(zc), _lib.MEMORY_DEVICE, ctypes.c_void_p(st)))
     return zc.value
 
@@ -347,7 +348,7 @@ class Coil:
     @staticmethod
     def _arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
                       primary_z_angles, secondary_y_angles, secondary_z_angles, precision_factor, compute_method,
-                      quantity):
+                      quantity, precision_mode=PrecisionMode.FP64):
         if ComputeMethod(compute_method) != ComputeMethod.GPU:
             raise NotImplementedError("this package provides the ComputeMethod.GPU path only")
         pp, sp = Coil._pair_args(primary, secondary, _factor(precision_factor))
@@ -356,19 +357,21 @@ class Coil:
         if len(ppose) != len(spose):
             raise ValueError("Array sizes do not match!")
         vals, _ = _pair_arrangements([primary.struct(pp)], secondary.struct(sp), [sp.to_struct()], ppose, spose,
-                                     quantity)
+                                     quantity, precision_mode)
         return vals
 
     @staticmethod
     def compute_all_mutual_inductance_arrangements(primary, secondary, primary_positions, secondary_positions,
                                                    primary_y_angles, primary_z_angles, secondary_y_angles,
                                                    secondary_z_angles, precision_factor=None,
-                                                   compute_method=ComputeMethod.GPU):
-        """Coil::computeAllMutualInductanceArrangements (ComputeMInductanceMethods.cxx:200-260): (n,) array."""
+                                                   compute_method=ComputeMethod.GPU,
+                                                   precision_mode=PrecisionMode.FP64):
+        """Coil::computeAllMutualInductanceArrangements (ComputeMInductanceMethods.cxx:200-260): (n,) array.
+        precision_mode FP32_COMPENSATED runs the primary quadrature in FP32 away from its winding."""
         return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
                                   primary_z_angles, secondary_y_angles, secondary_z_angles,
                                   precision_factor or PrecisionFactor(), compute_method,
-                                  _lib.PAIR_MUTUAL_INDUCTANCE)
+                                  _lib.PAIR_MUTUAL_INDUCTANCE, precision_mode)
 
     @staticmethod
     def compute_all_mutual_inductance_gradient_arrangements(primary, secondary, primary_positions,
@@ -386,12 +389,14 @@ class Coil:
     def compute_all_force_torque_arrangements(primary, secondary, primary_positions, secondary_positions,
                                               primary_y_angles, primary_z_angles, secondary_y_angles,
                                               secondary_z_angles, precision_factor=None,
-                                              compute_method=ComputeMethod.GPU):
+                                              compute_method=ComputeMethod.GPU,
+                                              precision_mode=PrecisionMode.FP64):
         """Coil::computeAllForceTorqueArrangements (ComputeForceMethods.cxx:189-248): (n, 6) array of
         force xyz and torque xyz on the secondary."""
         return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
                                   primary_z_angles, secondary_y_angles, secondary_z_angles,
-                                  precision_factor or PrecisionFactor(), compute_method, _lib.PAIR_FORCE_TORQUE)
+                                  precision_factor or PrecisionFactor(), compute_method, _lib.PAIR_FORCE_TORQUE,
+                                  precision_mode)
 
     def _pose_row(self):
         return self.get_position_vector(), self._s.y_axis_angle, self._s.z_axis_angle
@@ -485,7 +490,7 @@ class CoilGroup:
 
     # --- coil pairs: the secondary against every member except itself ---------------------
     def _group_arrangements(self, secondary, positions, y_angles, z_angles, precision_factor, compute_method,
-                            quantity):
+                            quantity, precision_mode=PrecisionMode.FP64):
         if ComputeMethod(compute_method) != ComputeMethod.GPU:
             raise NotImplementedError("this package provides the ComputeMethod.GPU path only")
         pf = _factor(precision_factor or PrecisionFactor())
@@ -497,22 +502,25 @@ class CoilGroup:
             prims.append(m.struct(pp))
             secs.append(sp.to_struct())
         spose = _poses(positions, y_angles, z_angles)
-        vals, _ = _pair_arrangements(prims, secondary.struct(), secs, None, spose, quantity)
+        vals, _ = _pair_arrangements(prims, secondary.struct(), secs, None, spose, quantity, precision_mode)
         return vals
 
     def compute_all_mutual_inductance_arrangements(self, secondary, secondary_positions, secondary_y_angles,
                                                    secondary_z_angles, precision_factor=None,
-                                                   compute_method=ComputeMethod.GPU):
+                                                   compute_method=ComputeMethod.GPU,
+                                                   precision_mode=PrecisionMode.FP64):
         """CoilGroup::computeAllMutualInductanceArrangements (ComputeMInductance.cxx:23-64)."""
         return self._group_arrangements(secondary, secondary_positions, secondary_y_angles, secondary_z_angles,
-                                        precision_factor, compute_method, _lib.PAIR_MUTUAL_INDUCTANCE)
+                                        precision_factor, compute_method, _lib.PAIR_MUTUAL_INDUCTANCE,
+                                        precision_mode)
 
     def compute_all_force_torque_arrangements(self, secondary, secondary_positions, secondary_y_angles,
                                               secondary_z_angles, precision_factor=None,
-                                              compute_method=ComputeMethod.GPU):
+                                              compute_method=ComputeMethod.GPU,
+                                              precision_mode=PrecisionMode.FP64):
         """CoilGroup::computeAllForceTorqueArrangements (ComputeForce.cxx:47-89): (n, 6)."""
         return self._group_arrangements(secondary, secondary_positions, secondary_y_angles, secondary_z_angles,
-                                        precision_factor, compute_method, _lib.PAIR_FORCE_TORQUE)
+                                        precision_factor, compute_method, _lib.PAIR_FORCE_TORQUE, precision_mode)
 
     def compute_mutual_inductance(self, secondary, precision_factor=None, compute_method=ComputeMethod.GPU):
         p, y, z = secondary._pose_row()

@@ -77,6 +77,10 @@ struct SegmentSet
 // Builds the segment list for `coils` (each at its own precision) for field
 // evaluation; precision selects whether FP32 tables are appended.
 bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err);
+// FP32 angular table of a coil at precision p (node order of the FP64 table)
+void buildPhi32(const PrecisionArgs &p, std::vector<PhiNode32> &out);
+// FP32 path's near-field box of a coil, into h.near_lo / near_hi / near_r2
+void setNearBox(const Coil &k, SegmentHeader &h);
 
 // host_coil.cpp
 const double *legendreNodes(int order);

@@ -1,326 +1,14 @@
 // FP32-compensated field kernels (included by fields.cu inside its anonymous
-// namespace, so they share the staging pipeline and the FP64 integrands).
-//
-// Arithmetic.  Per point and coil the frame transform, the per-thickness-node
-// constants and the final sums are FP64; the angular loop runs in FP32 with
-// Kahan-compensated accumulation per thickness node.  The FP32 integrands are
-// algebraic rewrites of the reference's (CalculateFieldsFast.cxx,
-// CalculateFieldsSlow.cxx) that remove every cancellation FP32 cannot afford:
-//   distance^2     D - 2 p r cos  ->  (p - r)^2 + z^2 + 2 p r (1 - cos)
-//   G2 - G1        -> dD G1^2 G2^2 / (G1 + G2),  dD = top^2 - bot^2 = 2 z b
-//   top G1 - bot G2 (point outside the slab |z| > b/2)
-//                  -> rho^2 dD G1^2 G2^2 / (top G1 + bot G2)
-//   asinh(top/rho) - asinh(bot/rho) (vector potential)
-//                  -> asinh(dD / (top s2 + bot s1)) outside the slab,
-//                     asinh((top s2 - bot s1) / rho^2) inside it
-//   RZ gradient node -> p cos (top G1^3 - bot G2^3) (equal node by node to the
-//                     reference's 1/M^2 form, without its cancellation)
-// and the azimuthal tables hold w*cos exactly antisymmetric about pi/2 in FP32.
+// namespace, so they share the staging pipeline and the FP64 integrands);
+// the integrands themselves are in integrands32.cuh.
 //
 // Near field.  A point inside a coil's winding box (inflated by a margin) is
-// not integrated here: its (point, segment) pair goes to a work list and a
-// second kernel evaluates it with the FP64 integrands, so warps never diverge
-// between the two paths.  If the list is full the pair is integrated in FP64
-// in place.
+// not integrated by the FP32 loop: its (point, segment) pair goes to a work
+// list and a second kernel evaluates it with the FP64 integrands, so warps
+// never diverge between the two paths.  If the list is full the pair is
+// integrated in FP64 in place.
 
-struct Kahan
-{
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x)
-    {
-        float y = x - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
-};
-
-// Runs body(k, accumulator set) over the angular nodes lane, lane + LANES, ...,
-// alternating between two independent accumulator sets so consecutive nodes do
-// not wait on each other's compensated additions.
-template <int LANES, typename Acc, typename Body>
-__device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body body)
-{
-    int k = lane;
-    for (; k + LANES < n; k += 2 * LANES)
-    {
-        body(k, a0);
-        body(k + LANES, a1);
-    }
-    if (k < n)
-        body(k, a0);
-}
-
-struct Acc1
-{
-    Kahan v;
-};
-struct Acc2
-{
-    Kahan h, z;
-};
-struct Acc4
-{
-    Kahan a, b, c, d;
-};
-
-// reciprocal: MUFU estimate (within 1 ulp), no special-case handling needed
-// since every argument here is a positive normal number
-__device__ __forceinline__ float rcpApprox(float x)
-{
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// reciprocal square root: the MUFU estimate (relative error below 2^-22.9); a
-// Newton-Raphson step (CCOIL_RSQRT_NEWTON=1) did not change the measured error
-// of the sums, which is set by the far-field cancellation, and costs 4 FMA per call
-#ifndef CCOIL_RSQRT_NEWTON
-#define CCOIL_RSQRT_NEWTON 0
-#endif
-__device__ __forceinline__ float rsqrtNR(float x)
-{
-    float y = rsqrtf(x);
-#if CCOIL_RSQRT_NEWTON
-    float e = fmaf(-x * y, y, 1.0f);
-    y = fmaf(0.5f * y, e, y);
-#endif
-    return y;
-}
-
-// asinh(u): the Maclaurin series sum_n (-1)^n (2n)! / (4^n (n!)^2 (2n+1)) u^(2n+1)
-// through n = 6 when every lane of the warp has |u| < 0.25 (truncation below
-// 6e-11 relative there), CUDA's asinhf otherwise
-__device__ __forceinline__ float asinhSmall(float u)
-{
-    const float u2 = u * u;
-    float p = 0.017352764f;          // 231/13312
-    p = fmaf(p, u2, -0.022372159f);  // -63/2816
-    p = fmaf(p, u2, 0.030381944f);   // 35/1152
-    p = fmaf(p, u2, -0.044642857f);  // -5/112
-    p = fmaf(p, u2, 0.075f);         // 3/40
-    p = fmaf(p, u2, -0.16666667f);   // -1/6
-    return fmaf(p * u2, u, u);
-}
-
-__device__ __forceinline__ float asinhFast(float u)
-{
-    const bool small = fabsf(u) < 0.25f;
-    if (__all_sync(__activemask(), small))
-        return asinhSmall(u);
-    return small ? asinhSmall(u) : asinhf(u);
-}
-
-__device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame &f)
-{
-    return f.r > h.near_lo[0] && f.r < h.near_hi[0] && f.z > h.near_lo[1] && f.z < h.near_hi[1];
-}
-
-template <int LANES>
-__device__ __forceinline__ double segmentA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                             const PhiNode32 *pn, const Frame &f, int lane)
-{
-    double sum = 0.0;
-    if (h.fast)
-    {
-        const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        const bool same = top * bot > 0.0;
-        const float topf = (float)top, botf = (float)bot;
-        const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * f.r);
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            Acc1 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc1 &acc) {
-                const PhiNode32 nd = pn[k];
-                const float rho2 = fmaf(b2, nd.omc, qf);
-                const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
-                const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
-                const float a = topf * s2, b = botf * s1;
-                const float num = same ? dDf : (a - b);
-                const float den = same ? (a + b) : rho2;
-                acc.v.add(nd.wc * asinhFast(num * rcpApprox(den)));
-            });
-            sum += t.y * t.x * (a0.v.value() + a1.v.value());
-        }
-    }
-    else
-    {
-        for (int i = 0; i < h.n_l; ++i)
-        {
-            const double2 l = lt[i];
-            const double zl = l.x + f.z;
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const float qf = (float)((t.x - f.r) * (t.x - f.r) + zl * zl), b2 = (float)(2.0 * t.x * f.r);
-                Acc1 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc1 &acc) {
-                    const PhiNode32 nd = pn[k];
-                    acc.v.add(nd.wc * rsqrtNR(fmaf(b2, nd.omc, qf)));
-                });
-                sum += l.y * t.y * t.x * (a0.v.value() + a1.v.value());
-            }
-        }
-    }
-    return sum;
-}
-
-template <int LANES>
-__device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                           const PhiNode32 *pn, const Frame &f, int lane, double &H, double &Z)
-{
-    H = 0.0;
-    Z = 0.0;
-    if (h.fast)
-    {
-        const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        const bool same = top * bot > 0.0;
-        const float topf = (float)top, botf = (float)bot;
-        const double dD = 2.0 * f.z * (2.0 * h.half_length);
-        const float dDf = (float)dD;
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * f.r);
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            // p^2 - p r cos = p (p - r) + p r (1 - cos)
-            const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-            Acc2 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc2 &acc) {
-                const PhiNode32 nd = pn[k];
-                const float rho2 = fmaf(b2, nd.omc, qf);
-                const float g1 = rsqrtNR(fmaf(b2, nd.omc, d1)), g2 = rsqrtNR(fmaf(b2, nd.omc, d2));
-                const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
-                const float t1 = topf * g1, t2 = botf * g2;
-                const float X = same ? (t1 + t2) : rho2;
-                const float Y = same ? dDf * gg2 : (t1 - t2);
-                const float R = rcpApprox(s * X);
-                const float num = fmaf(n1, nd.omc, n0);
-                acc.h.add(nd.wc * gg2 * (X * R));
-                acc.z.add(nd.w * num * Y * (s * R));
-            });
-            H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
-            Z += t.y * (a0.z.value() + a1.z.value());
-        }
-    }
-    else
-    {
-        for (int i = 0; i < h.n_l; ++i)
-        {
-            const double2 l = lt[i];
-            const double zl = l.x + f.z;
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const float qf = (float)((t.x - f.r) * (t.x - f.r) + zl * zl), b2 = (float)(2.0 * t.x * f.r);
-                const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-                Acc2 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc2 &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf));
-                    const float g3 = g * g * g;
-                    acc.z.add(nd.w * g3 * fmaf(n1, nd.omc, n0));
-                    acc.h.add(nd.wc * g3);
-                });
-                const double w = l.y * t.y;
-                H += w * t.x * zl * (a0.h.value() + a1.h.value());
-                Z += w * (a0.z.value() + a1.z.value());
-            }
-        }
-    }
-}
-
-// {RPhi, RR, RZ, ZZ}
-template <int LANES>
-__device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                           const PhiNode32 *pn, const Frame &f, int lane, double *g)
-{
-    double rphi = 0.0, rr = 0.0, rz = 0.0, zz = 0.0;
-    const double r = f.r;
-    if (h.fast)
-    {
-        const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        const bool same = top * bot > 0.0;
-        const float topf = (float)top, botf = (float)bot, lenf = (float)(2.0 * h.half_length);
-        const double dD = 2.0 * f.z * (2.0 * h.half_length);
-        const float dDf = (float)dD;
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - r) * (t.x - r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * r);
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            const float pf = (float)t.x, rf = (float)r;
-            const float rmp = (float)(r - t.x), pmr = (float)(t.x - r);
-            Acc4 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc4 &acc) {
-                const PhiNode32 nd = pn[k];
-                const float g1 = rsqrtNR(fmaf(b2, nd.omc, d1)), g2 = rsqrtNR(fmaf(b2, nd.omc, d2));
-                const float gg = g1 * g2, s = g1 + g2;
-                const float dg = dDf * gg * gg * rcpApprox(s);       // G2 - G1
-                const float dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));  // G1^3 - G2^3
-                const float g13 = g1 * g1 * g1;
-                const float rzv = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
-                acc.a.add(nd.wc * dg);
-                acc.b.add(nd.wc * fmaf(pf, nd.omc, rmp) * dg3);   // (r - p cos)
-                acc.d.add(nd.w * fmaf(rf, nd.omc, pmr) * dg3);    // (p - r cos)
-                acc.c.add(nd.wc * rzv);
-            });
-            const double w = t.y * t.x;
-            rphi += w / r * (a0.a.value() + a1.a.value());
-            rr += w * (a0.b.value() + a1.b.value());
-            zz += w * (a0.d.value() + a1.d.value());
-            rz += w * (a0.c.value() + a1.c.value());
-        }
-    }
-    else
-    {
-        for (int i = 0; i < h.n_l; ++i)
-        {
-            const double2 l = lt[i];
-            const double zl = l.x + f.z;
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const double p = t.x;
-                const float qf = (float)((p - r) * (p - r) + zl * zl), b2 = (float)(2.0 * p * r);
-                const float pf = (float)p, rf = (float)r;
-                const float rmp = (float)(r - p), pmr = (float)(p - r);
-                // RZ node G^5 (p cos (2p^2 + 2r^2 - zl^2 - p r cos) - 3 p^2 r) rewritten as
-                // -p G^5 (cos D + 3 (p - r cos)(r - p cos)), D the squared distance:
-                // no cancellation where the point approaches the ring (D -> 0)
-                Acc4 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc4 &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float den = fmaf(b2, nd.omc, qf);
-                    const float gq = rsqrtNR(den);
-                    const float g3 = gq * gq * gq, g5 = g3 * gq * gq;
-                    const float rpc = fmaf(pf, nd.omc, rmp), prc = fmaf(rf, nd.omc, pmr);
-                    acc.a.add(nd.wc * g3);
-                    acc.b.add(nd.wc * g5 * rpc);
-                    acc.d.add(nd.w * g5 * prc);
-                    acc.c.add(nd.w * g5 * fmaf(nd.c, den, 3.0f * prc * rpc));
-                });
-                const double w = l.y * t.y;
-                rphi += w * p * zl / r * (a0.a.value() + a1.a.value());
-                rr += -3.0 * w * p * zl * (a0.b.value() + a1.b.value());
-                zz += -3.0 * w * p * zl * (a0.d.value() + a1.d.value());
-                rz += -w * p * (a0.c.value() + a1.c.value());
-            }
-        }
-    }
-    g[0] = rphi;
-    g[1] = rr;
-    g[2] = rz;
-    g[3] = zz;
-}
+#include "integrands32.cuh"
 
 template <int FIELD, int LANES>
 __device__ __forceinline__ void integrateSegment32(const unsigned char *seg, const Frame &f, int lane, double *acc)

@@ -32,6 +32,7 @@ namespace ccoil
 namespace
 {
 #include "integrands64.cuh"
+#include "integrands32.cuh"
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kMuReduced = 1e-7;
@@ -194,10 +195,55 @@ struct WarpPose
     double offset, ablk;         // secondary azimuth offset and angular block size
 };
 
+// FP64 primary quadrature at one secondary node, out of line for the FP32
+// kernel (which takes it only for near-field nodes) so that its register
+// budget does not carry the FP64 integrands
+__device__ __noinline__ double pairA64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                       const double2 *pt, const Frame &f)
+{
+    return segmentA64<1>(h, tt, lt, pt, f, 0);
+}
+
+__device__ __noinline__ double2 pairB64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                        const double2 *pt, const Frame &f)
+{
+    double H, Z;
+    segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
+    return make_double2(H, Z);
+}
+
+// The FP32 primary quadrature, out of line as well: the call saves the
+// secondary-node state once per node, and the loop over the primary's nodes
+// gets the whole register budget
+__device__ __noinline__ double pairA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                       const PhiNode32 *pn, const Frame &f)
+{
+    return segmentA32<1>(h, tt, lt, pn, f, 0);
+}
+
+__device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                        const PhiNode32 *pn, const Frame &f)
+{
+    double H, Z;
+    segmentB32<1>(h, tt, lt, pn, f, 0, H, Z);
+    return make_double2(H, Z);
+}
+
+// 1: the FP64 kernel calls the out-of-line FP64 quadrature too
+#ifndef CCOIL_PAIR_CALL_FP64
+#define CCOIL_PAIR_CALL_FP64 0
+#endif
+
 // stagedBytes > 0: there is one primary and its whole pair blob (stagedBytes,
 // a multiple of 16) is copied into shared memory once per CTA, so the inner
-// quadrature reads its tables from shared memory instead of through L1
-template <int QTY>
+// quadrature reads its tables from shared memory instead of through L1.
+//
+// FP32 (mutual inductance and force/torque only): the primary quadrature at a
+// secondary node runs in the FP32-compensated integrands, except for the warp
+// iterations in which some lane's node lies in the primary's near-field box,
+// which take the FP64 integrands (warp-uniform, so lanes do not diverge); the
+// secondary-node sums and the cross-lane reduction stay FP64.
+template <int QTY, bool FP32>
 __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
                  const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
@@ -236,6 +282,8 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
             const double2 *st = reinterpret_cast<const double2 *>(base) + ph.off_st;
             const SecAngular *sa = reinterpret_cast<const SecAngular *>(reinterpret_cast<const double2 *>(base) +
                                                                         ph.off_sa);
+            const PhiNode32 *pn = reinterpret_cast<const PhiNode32 *>(reinterpret_cast<const double2 *>(base) +
+                                                                      h.off_f32);
             __syncwarp();  // every lane is done with the previous pose
             if (lane == 0)
             {
@@ -292,8 +340,12 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
 #pragma unroll
             for (int i = 0; i < W; ++i)
                 part[i] = 0.0;
-            for (int n = lane; n < nsec; n += 32)
+            // every lane runs the same number of iterations (warp-uniform choices
+            // below); a lane past the end evaluates the last node and drops it
+            for (int n0 = 0; n0 < nsec; n0 += 32)
             {
+                const bool valid = n0 + lane < nsec;
+                const int n = valid ? n0 + lane : nsec - 1;
                 const int k = n % ph.s_na, lt_i = n / ph.s_na;
                 const int t = lt_i % ph.s_nt, l = lt_i / ph.s_nt;
                 const double2 L = sl[l], R = st[t];
@@ -309,13 +361,21 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                                      S.sp[1] + L.x * sA * sB + R.x * ringP[1], S.sp[2] + L.x * cA + R.x * ringP[2]};
                 const double w = 0.125 * R.x * L.y * R.y * A.w;
                 const Frame f = toCoilFrameAt(S.pos, S.Ti, q[0], q[1], q[2]);
+                const bool far = !FP32 || !__any_sync(0xffffffffu, valid && nearWinding(h, f));
                 if (QTY == 0)
                 {
-                    const double av = segmentA64<1>(h, tt, lt, pt, f, 0);
+                    double av;
+                    if (!FP32)
+                        av = CCOIL_PAIR_CALL_FP64 ? pairA64(h, tt, lt, pt, f) : segmentA64<1>(h, tt, lt, pt, f, 0);
+                    else if (far)
+                        av = pairA32(h, tt, lt, pn, f);
+                    else
+                        av = pairA64(h, tt, lt, pt, f);
                     const double vx = -av * f.sphi, vy = av * f.cphi;
                     const double Ax = S.T[0] * vx + S.T[1] * vy, Ay = S.T[3] * vx + S.T[4] * vy,
                                  Az = S.T[6] * vx + S.T[7] * vy;
-                    part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
+                    if (valid)
+                        part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
                 }
                 else if (QTY == 2)
                 {
@@ -336,13 +396,21 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                         v[i] = J[i] * u[0] + J[3 + i] * u[1] + J[6 + i] * u[2];           // J^T u
                     for (int i = 0; i < 3; ++i)
                         o[i] = S.T[3 * i] * v[0] + S.T[3 * i + 1] * v[1] + S.T[3 * i + 2] * v[2];
-                    for (int i = 0; i < 3; ++i)
-                        part[i] += o[i] * w;
+                    if (valid)
+                        for (int i = 0; i < 3; ++i)
+                            part[i] += o[i] * w;
                 }
                 else
                 {
                     double H, Z;
-                    segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
+                    if (!FP32 && !CCOIL_PAIR_CALL_FP64)
+                        segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
+                    else
+                    {
+                        const double2 hz = FP32 && far ? pairB32(h, tt, lt, pn, f) : pairB64(h, tt, lt, pt, f);
+                        H = hz.x;
+                        Z = hz.y;
+                    }
                     const double vx = H * f.cphi, vy = H * f.sphi;
                     const double B[3] = {S.T[0] * vx + S.T[1] * vy + S.T[2] * Z, S.T[3] * vx + S.T[4] * vy + S.T[5] * Z,
                                          S.T[6] * vx + S.T[7] * vy + S.T[8] * Z};
@@ -352,11 +420,12 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                         dF[i] *= w;
                     const double rel[3] = {q[0] - S.sp[0], q[1] - S.sp[1], q[2] - S.sp[2]};
                     cross3(rel, dF, dT);
-                    for (int i = 0; i < 3; ++i)
-                    {
-                        part[i] += dF[i];
-                        part[3 + i] += dT[i];
-                    }
+                    if (valid)
+                        for (int i = 0; i < 3; ++i)
+                        {
+                            part[i] += dF[i];
+                            part[3 + i] += dT[i];
+                        }
                 }
             }
 #pragma unroll
@@ -387,7 +456,7 @@ void put(std::vector<unsigned char> &blob, const void *p, size_t n)
 // Primary tables as the reference's field integrators lay them out
 // (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
 // cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
-bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa,
+bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa, bool fp32,
                std::vector<unsigned char> &blob, std::string &err)
 {
     if (!validArgs(pp) || !validArgs(spa))
@@ -481,6 +550,14 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     ph.off_sl = h.off_phi + h.n_phi;
     ph.off_st = ph.off_sl + ph.s_nl;
     ph.off_sa = ph.off_st + ph.s_nt;
+    std::vector<PhiNode32> p32;
+    if (fp32)
+    {
+        // FP32 angular table (16-byte entries) after the secondary tables
+        buildPhi32(pp, p32);
+        h.off_f32 = ph.off_sa + 2 * ph.s_na;
+        setNearBox(prim, h);
+    }
     const double blocks = double(spa.length_blocks) * spa.thickness_blocks * spa.angular_blocks;
     ph.m_factor = 2 * kPi * sec.num_turns / prim.current / blocks;
     ph.f_factor = 2 * kPi * (sec.current * sec.num_turns) / blocks;
@@ -493,6 +570,7 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     put(blob, sl_.data(), sizeof(double) * sl_.size());
     put(blob, st_.data(), sizeof(double) * st_.size());
     put(blob, sa_.data(), sizeof(SecAngular) * sa_.size());
+    put(blob, p32.data(), sizeof(PhiNode32) * p32.size());
     (void)start;
     return true;
 }
@@ -528,8 +606,11 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     if (quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE && quantity != CCOIL_PAIR_FORCE_TORQUE &&
         quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown pair quantity");
-    if (precision != CCOIL_PRECISION_FP64)
-        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "coil-pair arrangements are evaluated in FP64");
+    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    if (precision == CCOIL_PRECISION_FP32_COMPENSATED && quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "the mutual-inductance gradient is evaluated in FP64 only");
+    const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
     if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
     if (z_axis_count)
@@ -552,7 +633,7 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     for (int j = 0; j < primary_count; ++j)
     {
         offsets.push_back((long long)blob.size());
-        if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], blob, err))
+        if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], fp32, blob, err))
             return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
     }
     DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ;
@@ -597,18 +678,24 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     if (blocks > 148LL * 64)
         blocks = 148LL * 64;
     auto *zc = static_cast<unsigned long long *>(dZ.p);
-    if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
-        pairKernel64<0><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
-            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
-            secP, count, o, zc, stagedBytes);
+    const auto *dB = static_cast<const unsigned char *>(dBlob.p);
+    const auto *dO = static_cast<const long long *>(dOff.p);
+    const size_t smem = (size_t)stagedBytes;
+    if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE && !fp32)
+        pairKernel64<0, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                     stagedBytes);
+    else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
+        pairKernel64<0, true><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                    stagedBytes);
+    else if (quantity == CCOIL_PAIR_FORCE_TORQUE && !fp32)
+        pairKernel64<1, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                     stagedBytes);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
-        pairKernel64<1><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
-            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
-            secP, count, o, zc, stagedBytes);
+        pairKernel64<1, true><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                    stagedBytes);
     else
-        pairKernel64<2><<<(unsigned)blocks, 128, (size_t)stagedBytes, st>>>(
-            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), primary_count, primP,
-            secP, count, o, zc, stagedBytes);
+        pairKernel64<2, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                     stagedBytes);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return cudaFail(e, "pair kernel launch");

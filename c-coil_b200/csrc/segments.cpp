@@ -46,6 +46,60 @@ void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
 }
 } // namespace
 
+// The FP32 angular table: cos(phi) built to be exactly antisymmetric about
+// pi/2 (node j and its mirror n-1-j), so the FP32 sum of w*cos over the nodes
+// vanishes exactly, and 1 - cos(phi) from a half-angle sine (no cancellation
+// near phi = 0).  Node order is that of the FP64 table.
+void buildPhi32(const PrecisionArgs &p, std::vector<PhiNode32> &phi32)
+{
+    const double aBlock = kPi / p.angular_blocks;
+    const double *ax = legendreNodes(p.angular_increments), *aw = legendreWeights(p.angular_increments);
+    const int n = p.angular_blocks * p.angular_increments;
+    phi32.assign(n, PhiNode32{});
+    for (int j = 0; j < n; ++j)
+    {
+        int bp = j / p.angular_increments, i = j % p.angular_increments;
+        double phi = aBlock * (bp + 0.5) + (aBlock * 0.5) * ax[i];
+        int m = n - 1 - j;  // mirror node
+        int mbp = m / p.angular_increments, mi = m % p.angular_increments;
+        double mphi = aBlock * (mbp + 0.5) + (aBlock * 0.5) * ax[mi];
+        // symmetric definition: c(j) = (cos(phi_j) - cos(phi_m)) / 2
+        double c = 0.5 * (std::cos(phi) - std::cos(mphi));
+        double s = std::sin(0.5 * phi);
+        phi32[j].c = (float)c;
+        phi32[j].w = (float)aw[i];
+        phi32[j].wc = (float)(aw[i] * c);
+        phi32[j].omc = (float)(2.0 * s * s);
+    }
+    for (int j = 0; j < n; ++j)
+    {
+        // force exact antisymmetry of the FP32 values
+        int m = n - 1 - j;
+        if (m < j)
+        {
+            phi32[j].c = -phi32[m].c;
+            phi32[j].wc = -phi32[m].wc;
+        }
+        else if (m == j)
+        {
+            phi32[j].c = 0.0f;
+            phi32[j].wc = 0.0f;
+        }
+    }
+}
+
+// Near-field region of the FP32 path: the winding's cross-section box in
+// (r, z), inflated by a margin; points inside are integrated in FP64.
+void setNearBox(const Coil &k, SegmentHeader &h)
+{
+    const double margin = nearMargin() * k.inner_radius;
+    h.near_lo[0] = k.inner_radius - margin;
+    h.near_hi[0] = k.inner_radius + k.thickness + margin;
+    h.near_lo[1] = -0.5 * k.length - margin;
+    h.near_hi[1] = 0.5 * k.length + margin;
+    h.near_r2 = margin * margin;
+}
+
 bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err)
 {
     out.blob.clear();
@@ -111,45 +165,7 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
                 phiNodes.push_back({std::cos(blockPos + (aBlock * 0.5) * ax[i]), aw[i]});
         }
         if (fp32)
-        {
-            // The FP32 tables use cos(phi) built to be exactly antisymmetric about
-            // pi/2 (node j and its mirror n-1-j), so the FP32 sum of w*cos over
-            // the nodes vanishes exactly, and 1 - cos(phi) from a half-angle sine
-            // (no cancellation near phi = 0).
-            const int n = (int)phiNodes.size();
-            phi32.resize(n);
-            for (int j = 0; j < n; ++j)
-            {
-                int bp = j / p.angular_increments, i = j % p.angular_increments;
-                double phi = aBlock * (bp + 0.5) + (aBlock * 0.5) * ax[i];
-                int m = n - 1 - j;  // mirror node
-                int mbp = m / p.angular_increments, mi = m % p.angular_increments;
-                double mphi = aBlock * (mbp + 0.5) + (aBlock * 0.5) * ax[mi];
-                // symmetric definition: c(j) = (cos(phi_j) - cos(phi_m)) / 2
-                double c = 0.5 * (std::cos(phi) - std::cos(mphi));
-                double s = std::sin(0.5 * phi);
-                float cf = (float)c;
-                phi32[j].c = cf;
-                phi32[j].w = (float)aw[i];
-                phi32[j].wc = (float)(aw[i] * c);
-                phi32[j].omc = (float)(2.0 * s * s);
-            }
-            for (int j = 0; j < n; ++j)
-            {
-                // force exact antisymmetry of the FP32 values
-                int m = n - 1 - j;
-                if (m < j)
-                {
-                    phi32[j].c = -phi32[m].c;
-                    phi32[j].wc = -phi32[m].wc;
-                }
-                else if (m == j)
-                {
-                    phi32[j].c = 0.0f;
-                    phi32[j].wc = 0.0f;
-                }
-            }
-        }
+            buildPhi32(p, phi32);
 
         const int headerBytes = (int)sizeof(SegmentHeader);
         const int fixedBytes = headerBytes + 16 * (int)(tNodes.size() + lNodes.size());
@@ -180,14 +196,7 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
             h.off_l = h.off_t + h.n_t;
             h.off_phi = h.off_l + h.n_l;
             h.off_f32 = fp32 ? h.off_phi + cnt : 0;
-            // near-field region of the FP32 path: the winding's cross-section box in
-            // (r, z), inflated by a margin; points inside go to the FP64 loop
-            double margin = nearMargin() * k.inner_radius;
-            h.near_lo[0] = k.inner_radius - margin;
-            h.near_hi[0] = k.inner_radius + k.thickness + margin;
-            h.near_lo[1] = -0.5 * k.length - margin;
-            h.near_hi[1] = 0.5 * k.length + margin;
-            h.near_r2 = margin * margin;
+            setNearBox(k, h);
 
             SegmentDesc d;
             d.offset = (long long)out.blob.size();

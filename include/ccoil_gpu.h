@@ -204,7 +204,13 @@ typedef struct ccoil_pose
  * (src/Coil/CUDAKernels/CoilAcceleration.h:21-29,
  * src/CoilGroup/CUDAKernels/CoilGroupAcceleration.h:27-37).
  * Arrangements that are exact z-axis cases (Coil::isZAxisCase) are evaluated
- * with the general formula; their number is returned in *z_axis_count. */
+ * with the general formula; their number is returned in *z_axis_count.
+ * precision: CCOIL_PRECISION_FP64 follows the reference's double arithmetic;
+ * CCOIL_PRECISION_FP32_COMPENSATED (mutual inductance and force/torque only;
+ * CCOIL_ERR_NOT_SUPPORTED for the gradient) evaluates the primary's quadrature
+ * in FP32 with compensated sums, except where a secondary node lies within the
+ * primary's near-field box (winding cross-section inflated by 0.1 R), which
+ * is evaluated in FP64; sums over secondary nodes and primaries are FP64. */
 int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
                             const ccoil_precision_args_t *secondary_precisions, const ccoil_pose_t *primary_poses,
                             const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
