@@ -116,7 +116,47 @@ def pair_setup(cc, workloads, n, seed):
     return prim_row, sec_row, prim.struct(pp), sec.struct(sp), sp.to_struct(), pposes, sposes, (pp, sp)
 
 
-def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier):
+def rel_err_stats(got, ref, mask=None):
+    """Relative error per row (norm-wise), the denominator floored at 1e-3 x the
+    batch's largest reference norm; median, 99th percentile and maximum, over all
+    rows or over `mask`."""
+    import torch
+    got = got.reshape(len(got), -1)
+    ref = ref.reshape(len(ref), -1)
+    nb = ref.norm(dim=1)
+    e = (got - ref).norm(dim=1) / torch.clamp(nb, min=1e-3 * float(nb.max()))
+    if mask is not None:
+        e = e[mask]
+    if e.numel() == 0:
+        return None
+    q = torch.quantile(e[:1 << 24].float(), torch.tensor([0.5, 0.99], device=e.device)).tolist()
+    return {"median": q[0], "p99": q[1], "max": float(e.max()), "rows": int(e.numel())}
+
+
+def winding_masks(rows, pts):
+    """Boolean masks over points (numpy, on the host): `near` = inside some coil's
+    near-field box (its winding cross-section in (r, z) inflated by 0.1 R), `band` =
+    radius, in some coil's frame, within [0.9 R, R + a + 0.1 R] at any z, where the
+    reference's gradient RZ integrand is ill-conditioned (its own FP64 result
+    carries ~1e-7 relative error there, so FP32 is judged outside it)."""
+    near = np.zeros(len(pts), dtype=bool)
+    band = np.zeros(len(pts), dtype=bool)
+    for row in rows:
+        R, a_, b_ = row[0], row[1], row[2]
+        yA, zA = row[9], row[10]
+        cY, sY, cZ, sZ = np.cos(yA), np.sin(yA), np.cos(zA), np.sin(zA)
+        Ti = np.array([[cZ * cZ * cY - sZ * sZ, sZ * cZ * cY + sZ * cZ, -cZ * sY],
+                       [-sZ * cZ * cY - sZ * cZ, cZ * cZ - sZ * sZ * cY, sZ * sY],
+                       [sY * cZ, sY * sZ, cY]])
+        d = (pts - row[6:9]) @ Ti.T
+        r = np.hypot(d[:, 0], d[:, 1])
+        inr = (r > 0.9 * R) & (r < R + a_ + 0.1 * R)
+        band |= inr
+        near |= inr & (np.abs(d[:, 2]) < 0.5 * b_ + 0.1 * R)
+    return near, band
+
+
+def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, modes):
     import torch
     from ccoil_b200.coil import pair_arrangements_device
     _, _, pstruct, sstruct, spre, pposes, sposes, (pp, sp) = pair_setup(cc, workloads, a.arrangements,
@@ -124,21 +164,30 @@ def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier):
     dp = torch.from_numpy(pposes).to(dev)
     ds = torch.from_numpy(sposes).to(dev)
     res = {}
-    for name, q, w in (("M", 0, 1), ("FT", 1, 6)):
-        out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
-        pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out)  # warm-up
-        torch.cuda.synchronize()
-        barrier()
-        ms = 0.0
-        for _ in range(a.steps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            zc = pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out)
-            e1.record()
+    for mode in modes:
+        key = "fp64" if int(mode) == 0 else "fp32c"
+        res[key] = {}
+        for name, q, w in (("M", 0, 1), ("FT", 1, 6)):
+            out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
+            pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out, precision_mode=mode)  # warm-up
             torch.cuda.synchronize()
-            ms += e0.elapsed_time(e1)
-        ms = max_over_ranks(ms / a.steps)
-        res[name] = {"ms": ms, "arrangements_per_s": a.arrangements / (ms * 1e-3), "z_axis_cases": zc}
+            barrier()
+            ms = 0.0
+            for _ in range(a.steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                zc = pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out, precision_mode=mode)
+                e1.record()
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+            ms = max_over_ranks(ms / a.steps)
+            res[key][name] = {"ms": ms, "arrangements_per_s": a.arrangements / (ms * 1e-3), "z_axis_cases": zc,
+                              "out": out}
+    if len(res) == 2:
+        m32, m64 = res["fp32c"]["M"]["out"], res["fp64"]["M"]["out"]
+        f32, f64 = res["fp32c"]["FT"]["out"], res["fp64"]["FT"]["out"]
+        res["errors"] = {"M": rel_err_stats(m32, m64), "F": rel_err_stats(f32[:, :3], f64[:, :3]),
+                         "T": rel_err_stats(f32[:, 3:], f64[:, 3:])}
     aB, tB, lB, aI, tI, lI = sp.as_tuple()
     res["secondary_nodes"] = aB * aI * tB * tI * lB * lI
     res["primary_nodes"] = pp.angular_blocks * pp.angular_increments * pp.thickness_blocks * pp.thickness_increments
@@ -313,13 +362,36 @@ def main():
     value = units_per_step / (r["step_ms"] * 1e-3)
     e2e_value = units_per_step / r["e2e_s"]
 
-    # roofline of the dominant kernel against the measured pipe peak
-    p64, p32, pmu = (ctypes_peaks(cc) if rank == 0 else (None, None, None))
+    # roofline of the dominant kernel: its pipe work (opcount's model, divide /
+    # square root / log charged at their measured FP64-pipe cost) over its
+    # CUDA-event time, against the measured peak of the pipe that binds it
+    rates = ctypes_rates(cc)
     dom = max(r["field_ms"], key=r["field_ms"].get)
     fidx = dict(FIELDS)[dom]
+    t_dom = r["field_ms"][dom] * 1e-3
     flops_launch = opcount.group_flops_per_point(fidx, coils) * a.points
-    achieved = flops_launch / (r["field_ms"][dom] * 1e-3) / 1e12
-    peak = p64 if headline_mode == 0 else p32
+    model = {"algorithmic_flops_per_launch": flops_launch, "algorithmic_tflops": flops_launch / t_dom / 1e12}
+    if rates is None:
+        bound, achieved, peak, unit = "unmeasured", None, None, "TFLOP/s"
+    elif headline_mode == 0:
+        slots = opcount.fp64_slots_per_point(fidx, coils, rates) * a.points
+        bound, unit = "fp64-pipe", "TFLOP/s"
+        achieved, peak = 2.0 * slots / t_dom / 1e12, 2.0 * rates[0] / 1e12
+        model.update({"fp64_pipe_slots_per_launch": slots,
+                      "dfma_slots_per_op": {"div": rates[0] / rates[1], "sqrt": rates[0] / rates[2],
+                                            "log": rates[0] / rates[3]}})
+    else:
+        ins, mufu = opcount.fp32_ops_per_point(fidx, coils)
+        ins, mufu = ins * a.points, mufu * a.points
+        issue, xu = ins / t_dom / rates[4], mufu / t_dom / rates[5]
+        if issue >= xu:
+            bound, unit = "fp32-issue", "TFLOP/s"
+            achieved, peak = 2.0 * ins / t_dom / 1e12, 2.0 * rates[4] / 1e12
+        else:
+            bound, unit = "xu (MUFU)", "Tops/s"
+            achieved, peak = mufu / t_dom / 1e12, rates[5] / 1e12
+        model.update({"fp32_instructions_per_launch": ins, "mufu_ops_per_launch": mufu,
+                      "fp32_issue_frac": issue, "mufu_frac": xu})
     traffic = read_traffic(dom, headline_mode)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -330,39 +402,58 @@ def main():
             "per_field_ms": r["field_ms"],
             "node_evals_per_s": opcount.group_nodes_per_point(coils) * a.points * world * len(FIELDS) /
             (r["step_ms"] * 1e-3),
-            "gpu_launches": a.steps * len(FIELDS),
+            "gpu_launches": a.steps * len(FIELDS) * (2 if headline_mode == 1 else 1),
             "clocks": r["clocks"],
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": len(FIELDS) * a.points * 24,
                     "d2h_bytes_per_step": sum(a.points * 8 * (9 if f == 3 else 3) for _, f in FIELDS)},
-            "roofline": {"bound": "fp64-pipe" if headline_mode == 0 else "fp32-pipe+xu", "kernel": "field %s" % dom,
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                         "peak_source": "measured on this GPU by ccoil_measure_pipe_peaks (FMA = 2 flops)",
-                         "flops_per_launch": flops_launch,
-                         "pipes_measured": {"fp64_tflops": p64, "fp32_tflops": p32, "mufu_rsqrt_tops": pmu}}}
+            "roofline": {"bound": bound, "kernel": "field %s" % dom, "achieved": achieved, "peak": peak,
+                         "unit": unit, "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                         "peak_source": "measured on this GPU by ccoil_measure_op_rates (FMA = 2 flops)",
+                         "model": model,
+                         "rates_measured": None if rates is None else {
+                             "fp64_fma_tflops": 2 * rates[0] / 1e12, "fp32_fma_tflops": 2 * rates[4] / 1e12,
+                             "mufu_tops": rates[5] / 1e12, "ddiv_gops": rates[1] / 1e9,
+                             "dsqrt_gops": rates[2] / 1e9, "dlog_gops": rates[3] / 1e9}}}
     if len(modes) == 2:
         r64 = results[0]
         line["fp64"] = {"value": units_per_step / (r64["step_ms"] * 1e-3), "ms_per_step": r64["step_ms"],
                         "per_field_ms": r64["field_ms"]}
         line["fp32c_speedup_vs_fp64"] = r64["step_ms"] / r["step_ms"]
-        errs = {}
+        near, band = (torch.from_numpy(m).to(dev) for m in winding_masks(rows, pts_host))
+        errs = {"definition": "norm-wise relative error per point, denominator floored at 1e-3 x the batch's "
+                              "largest FP64 norm; 'away' = outside every coil's winding box inflated by 0.1 R "
+                              "(for G also outside every coil's radial band [0.9 R, R + a + 0.1 R], where the "
+                              "reference's FP64 gradient is itself ill-conditioned)",
+                "away_fraction": {"A_B": float((~near).float().mean()), "G": float((~band).float().mean())}}
         for name, f in FIELDS:
-            e = (results[1]["outs"][name] - r64["outs"][name]).norm(dim=1) / r64["outs"][name].norm(dim=1)
-            errs[name] = {"max": float(e.max()), "median": float(e.median())}
+            away = ~band if f == 3 else ~near
+            errs[name] = {"all": rel_err_stats(results[1]["outs"][name], r64["outs"][name]),
+                          "away": rel_err_stats(results[1]["outs"][name], r64["outs"][name], away)}
         line["fp32c_rel_err_vs_fp64"] = errs
     if a.arrangements > 0:
-        arr = bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier)
+        arr = bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, modes)
+        head = "fp32c" if "fp32c" in arr else "fp64"
         line["arrangements"] = {"workload": "RECTANGULAR primary (0.1, 0.05, 0.1 m, N=200) x THIN secondary "
                                             "(0.05, 0, 0.2 m, N=100), %d arrangements per GPU, offsets in a "
-                                            "0.6 m cube, random orientations, 5%% near-coaxial, PF 5, FP64"
+                                            "0.6 m cube, random orientations, 5%% near-coaxial, PF 5"
                                             % a.arrangements,
-                                "M_arrangements_per_s": arr["M"]["arrangements_per_s"] * world,
-                                "FT_arrangements_per_s": arr["FT"]["arrangements_per_s"] * world,
-                                "M_ms": arr["M"]["ms"], "FT_ms": arr["FT"]["ms"],
+                                "precision_mode": head,
+                                "M_arrangements_per_s": arr[head]["M"]["arrangements_per_s"] * world,
+                                "FT_arrangements_per_s": arr[head]["FT"]["arrangements_per_s"] * world,
                                 "secondary_nodes": arr["secondary_nodes"], "primary_nodes": arr["primary_nodes"],
-                                "z_axis_cases": arr["M"]["z_axis_cases"]}
-        line["gpu_launches"] += 2 * a.steps
+                                "z_axis_cases": arr[head]["M"]["z_axis_cases"]}
+        for key in ("fp64", "fp32c"):
+            if key in arr:
+                line["arrangements"][key] = {
+                    "M_arrangements_per_s": arr[key]["M"]["arrangements_per_s"] * world,
+                    "FT_arrangements_per_s": arr[key]["FT"]["arrangements_per_s"] * world,
+                    "M_ms": arr[key]["M"]["ms"], "FT_ms": arr[key]["FT"]["ms"]}
+        if "errors" in arr:
+            line["arrangements"]["fp32c_speedup_vs_fp64"] = {
+                q: arr["fp64"][q]["ms"] / arr["fp32c"][q]["ms"] for q in ("M", "FT")}
+            line["arrangements"]["fp32c_rel_err_vs_fp64"] = arr["errors"]
+        line["gpu_launches"] += 2 * a.steps * len(modes)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, cores, dt, desc = cpu_reference_rate(a, a.cpu_sample_points)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
@@ -379,14 +470,14 @@ def main():
         dist.destroy_process_group()
 
 
-def ctypes_peaks(cc):
+def ctypes_rates(cc):
     import ctypes
     L = cc.lib()
-    L.ccoil_measure_pipe_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
-    v = [ctypes.c_double(), ctypes.c_double(), ctypes.c_double()]
-    if L.ccoil_measure_pipe_peaks(*[ctypes.byref(x) for x in v]) != 0:
-        return None, None, None
-    return v[0].value, v[1].value, v[2].value
+    L.ccoil_measure_op_rates.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    v = (ctypes.c_double * 6)()
+    if L.ccoil_measure_op_rates(v, 6) != 0:
+        return None
+    return list(v)
 
 
 def read_traffic(field, mode):

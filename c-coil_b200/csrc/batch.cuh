@@ -6,9 +6,9 @@
 // system, L lanes per point -- and sorts them longest first.  A grid sized to
 // the machine (CTAs per SM x 148) pulls items from an atomic counter until the
 // list is exhausted, so long items start first and short ones fill the tail.
-// An item stages its system's segments through the same double-buffered
-// TMA/mbarrier pipeline as the single-system kernels; the stage phases are
-// tracked across items.  In FP32_COMPENSATED mode near-field pairs go to the
+// An item reads its system's segment tables straight from global memory
+// (through L1, as the single-system kernels do), so warps synchronise only to
+// take the next item.  In FP32_COMPENSATED mode near-field pairs go to the
 // work list with the field in the top bits of the segment index.
 
 struct BatchItem
@@ -24,14 +24,8 @@ struct BatchItem
 
 constexpr int kFieldShift = 28;  // NearPair.segment = segment | field << 28
 
-struct StageState
-{
-    unsigned uses[kSegmentStages];  // completed uses per stage (uniform across the CTA)
-};
-
 template <int PREC, int FIELD, int LANES>
-__device__ __forceinline__ bool batchItem(const BatchItem &I, unsigned char *smem, unsigned long long *bars,
-                                          StageState &ss, int *timedOut, const unsigned char *__restrict__ blob,
+__device__ __forceinline__ void batchItem(const BatchItem &I, const unsigned char *__restrict__ blob,
                                           const SegmentDesc *__restrict__ segs, const double *__restrict__ points,
                                           double *__restrict__ out, NearPair *__restrict__ work,
                                           unsigned long long workCapacity, unsigned long long *__restrict__ workCount)
@@ -43,12 +37,6 @@ __device__ __forceinline__ bool batchItem(const BatchItem &I, unsigned char *sme
     const long long p = (long long)I.point_begin + local;
     const int nseg = I.seg_end - I.seg_begin;
 
-    if (threadIdx.x == 0)
-        for (int s = 0; s < kSegmentStages && s < nseg; ++s)
-        {
-            const SegmentDesc d = segs[I.seg_begin + s];
-            stageSegment(smem + s * kSegmentBytes, blob + d.offset, (unsigned)d.bytes, &bars[s]);
-        }
     double px = 0.0, py = 0.0, pz = 0.0;
     if (active)
     {
@@ -61,52 +49,36 @@ __device__ __forceinline__ bool batchItem(const BatchItem &I, unsigned char *sme
     for (int i = 0; i < W; ++i)
         acc[i] = 0.0;
 
-    for (int s = 0; s < nseg; ++s)
+    for (int s = 0; s < nseg && active; ++s)
     {
-        const int stage = s % kSegmentStages;
-        const bool ok = mbarWait(&bars[stage], ss.uses[stage] & 1u);
-        ss.uses[stage]++;
-        if (!ok)
-            *timedOut = 1;
-        if (active && ok)
+        const unsigned char *seg = blob + segs[I.seg_begin + s].offset;
+        if (PREC == CCOIL_PRECISION_FP64)
+            integrateSegment64<FIELD, LANES>(seg, px, py, pz, lane, acc);
+        else
         {
-            const unsigned char *seg = smem + stage * kSegmentBytes;
-            if (PREC == CCOIL_PRECISION_FP64)
-                integrateSegment64<FIELD, LANES>(seg, px, py, pz, lane, acc);
+            const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
+            const Frame f = toCoilFrame(h, px, py, pz);
+            if (!nearWinding(h, f))
+                integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
             else
             {
-                const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
-                const Frame f = toCoilFrame(h, px, py, pz);
-                if (!nearWinding(h, f))
-                    integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
-                else
+                bool queued = false;
+                if (lane == 0)
                 {
-                    bool queued = false;
-                    if (lane == 0)
+                    unsigned long long slot = atomicAdd(workCount, 1ull);
+                    if (slot < workCapacity)
                     {
-                        unsigned long long slot = atomicAdd(workCount, 1ull);
-                        if (slot < workCapacity)
-                        {
-                            work[slot].point = (int)p;
-                            work[slot].segment = (I.seg_begin + s) | (FIELD << kFieldShift);
-                            queued = true;
-                        }
+                        work[slot].point = (int)p;
+                        work[slot].segment = (I.seg_begin + s) | (FIELD << kFieldShift);
+                        queued = true;
                     }
-                    const unsigned groupMask = LANES == 32 ? 0xffffffffu
-                                                           : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
-                    queued = __shfl_sync(groupMask, queued, (threadIdx.x % 32) / LANES * LANES);
-                    if (!queued)
-                        integrateSegment64Fallback<FIELD, LANES>(seg, px, py, pz, lane, acc);
                 }
+                const unsigned groupMask = LANES == 32 ? 0xffffffffu
+                                                       : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
+                queued = __shfl_sync(groupMask, queued, (threadIdx.x % 32) / LANES * LANES);
+                if (!queued)
+                    integrateSegment64Fallback<FIELD, LANES>(seg, px, py, pz, lane, acc);
             }
-        }
-        __syncthreads();
-        if (*timedOut)
-            return false;
-        if (threadIdx.x == 0 && s + kSegmentStages < nseg)
-        {
-            const SegmentDesc d = segs[I.seg_begin + s + kSegmentStages];
-            stageSegment(smem + stage * kSegmentBytes, blob + d.offset, (unsigned)d.bytes, &bars[stage]);
         }
     }
 #pragma unroll
@@ -120,79 +92,48 @@ __device__ __forceinline__ bool batchItem(const BatchItem &I, unsigned char *sme
         for (int i = 0; i < W; ++i)
             out[W * p + i] = acc[i];
     }
-    return true;
 }
 
 template <int PREC, int FIELD>
-__device__ __forceinline__ bool batchItemLanes(const BatchItem &I, unsigned char *smem, unsigned long long *bars,
-                                               StageState &ss, int *timedOut, const unsigned char *blob,
-                                               const SegmentDesc *segs, const double *points, double *out,
-                                               NearPair *work, unsigned long long cap, unsigned long long *count)
+__device__ __forceinline__ void batchItemLanes(const BatchItem &I, const unsigned char *blob, const SegmentDesc *segs,
+                                               const double *points, double *out, NearPair *work,
+                                               unsigned long long cap, unsigned long long *count)
 {
     switch (I.lanes)
     {
-        case 1: return batchItem<PREC, FIELD, 1>(I, smem, bars, ss, timedOut, blob, segs, points, out, work, cap, count);
-        case 4: return batchItem<PREC, FIELD, 4>(I, smem, bars, ss, timedOut, blob, segs, points, out, work, cap, count);
-        default:
-            return batchItem<PREC, FIELD, 32>(I, smem, bars, ss, timedOut, blob, segs, points, out, work, cap, count);
+        case 1: batchItem<PREC, FIELD, 1>(I, blob, segs, points, out, work, cap, count); break;
+        case 4: batchItem<PREC, FIELD, 4>(I, blob, segs, points, out, work, cap, count); break;
+        default: batchItem<PREC, FIELD, 32>(I, blob, segs, points, out, work, cap, count); break;
     }
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(128) batchKernel(const unsigned char *__restrict__ blob,
-                                                   const SegmentDesc *__restrict__ segs,
-                                                   const BatchItem *__restrict__ items, int nitems,
-                                                   unsigned *__restrict__ next, const double *__restrict__ points,
-                                                   double *__restrict__ outA, double *__restrict__ outB,
-                                                   double *__restrict__ outG, NearPair *__restrict__ work,
-                                                   unsigned long long workCapacity,
-                                                   unsigned long long *__restrict__ workCount)
+__global__ void __launch_bounds__(128, 5) batchKernel(const unsigned char *__restrict__ blob,
+                                                      const SegmentDesc *__restrict__ segs,
+                                                      const BatchItem *__restrict__ items, int nitems,
+                                                      unsigned *__restrict__ next, const double *__restrict__ points,
+                                                      double *__restrict__ outA, double *__restrict__ outB,
+                                                      double *__restrict__ outG, NearPair *__restrict__ work,
+                                                      unsigned long long workCapacity,
+                                                      unsigned long long *__restrict__ workCount)
 {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long bars[kSegmentStages];
     __shared__ int itemIndex;
-    __shared__ int timedOut;
-    if (threadIdx.x == 0)
-    {
-        timedOut = 0;
-        for (int s = 0; s < kSegmentStages; ++s)
-            mbarInit(&bars[s], 1);
-        fenceBarrierInit();
-    }
-    StageState ss;
-    for (int s = 0; s < kSegmentStages; ++s)
-        ss.uses[s] = 0;
     for (;;)
     {
         if (threadIdx.x == 0)
             itemIndex = (int)atomicAdd(next, 1u);
         __syncthreads();
         const int it = itemIndex;
+        __syncthreads();  // every thread has read the index before it is replaced
         if (it >= nitems)
             break;
         const BatchItem I = items[it];
-        bool ok;
         if (I.field == CCOIL_FIELD_B)
-            ok = batchItemLanes<PREC, CCOIL_FIELD_B>(I, smem, bars, ss, &timedOut, blob, segs, points, outB, work,
-                                                     workCapacity, workCount);
+            batchItemLanes<PREC, CCOIL_FIELD_B>(I, blob, segs, points, outB, work, workCapacity, workCount);
         else if (I.field == CCOIL_FIELD_G)
-            ok = batchItemLanes<PREC, CCOIL_FIELD_G>(I, smem, bars, ss, &timedOut, blob, segs, points, outG, work,
-                                                     workCapacity, workCount);
+            batchItemLanes<PREC, CCOIL_FIELD_G>(I, blob, segs, points, outG, work, workCapacity, workCount);
         else
-            ok = batchItemLanes<PREC, CCOIL_FIELD_A>(I, smem, bars, ss, &timedOut, blob, segs, points, outA, work,
-                                                     workCapacity, workCount);
-        if (!ok)
-        {
-            if (threadIdx.x == 0)
-            {
-                atomicAdd(&g_timeouts, 1ull);
-                // drain the stages still in flight (bounded)
-                for (int t = 0; t < kSegmentStages; ++t)
-                    mbarWait(&bars[t], ss.uses[t] & 1u);
-            }
-            return;
-        }
-        __syncthreads();  // the next item may restage both buffers
+            batchItemLanes<PREC, CCOIL_FIELD_A>(I, blob, segs, points, outA, work, workCapacity, workCount);
     }
 }
 
@@ -259,15 +200,14 @@ int launchBatchImpl(const BatchLaunch &B, cudaStream_t st)
         return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     if (B.nitems == 0)
         return CCOIL_OK;
-    const size_t smem = (size_t)kSegmentStages * kSegmentBytes;
     NearPair *work = reinterpret_cast<NearPair *>(B.d_work);
     const BatchItem *items = static_cast<const BatchItem *>(B.d_items);
     if (B.precision == CCOIL_PRECISION_FP64)
-        batchKernel<CCOIL_PRECISION_FP64><<<B.grid, 128, smem, st>>>(B.d_blob, B.d_segs, items, B.nitems, B.d_next,
+        batchKernel<CCOIL_PRECISION_FP64><<<B.grid, 128, 0, st>>>(B.d_blob, B.d_segs, items, B.nitems, B.d_next,
                                                                      B.d_points, B.d_outA, B.d_outB, B.d_outG, work,
                                                                      B.work_capacity, B.d_work_count);
     else
-        batchKernel<CCOIL_PRECISION_FP32_COMPENSATED><<<B.grid, 128, smem, st>>>(
+        batchKernel<CCOIL_PRECISION_FP32_COMPENSATED><<<B.grid, 128, 0, st>>>(
             B.d_blob, B.d_segs, items, B.nitems, B.d_next, B.d_points, B.d_outA, B.d_outB, B.d_outG, work,
             B.work_capacity, B.d_work_count);
     e = cudaGetLastError();

@@ -84,8 +84,19 @@ __device__ __forceinline__ bool mbarWait(unsigned long long *bar, unsigned parit
 
 #include "integrands64.cuh"
 
+// 6 CTAs of 128 threads per SM (80 registers; measured best on B200)
+#ifndef CCOIL_FP64_MIN_BLOCKS
+#define CCOIL_FP64_MIN_BLOCKS 6
+#endif
+// 1: segments staged into shared memory (double-buffered bulk copies, one CTA
+// barrier per segment); 0 (default): each warp reads the tables from global
+// memory through L1, with no barrier between warps
+#ifndef CCOIL_FP64_STAGE
+#define CCOIL_FP64_STAGE 0
+#endif
+
 template <int FIELD, int LANES>
-__global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__restrict__ blob,
+__global__ void __launch_bounds__(128, CCOIL_FP64_MIN_BLOCKS) fieldsKernel64(const unsigned char *__restrict__ blob,
                                                       const SegmentDesc *__restrict__ segs, int nseg,
                                                       const double *__restrict__ points, long long npts,
                                                       double *__restrict__ out)
@@ -98,6 +109,7 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
     const long long p = (long long)blockIdx.x * (blockDim.x / LANES) + threadIdx.x / LANES;
     const bool active = p < npts;
 
+#if CCOIL_FP64_STAGE
     if (threadIdx.x == 0)
     {
         for (int s = 0; s < kSegmentStages; ++s)
@@ -107,6 +119,7 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
             stageSegment(smem + s * kSegmentBytes, blob + segs[s].offset, (unsigned)segs[s].bytes, &bars[s]);
     }
     __syncthreads();
+#endif
 
     double px = 0.0, py = 0.0, pz = 0.0;
     if (active)
@@ -122,6 +135,10 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
 
     for (int s = 0; s < nseg; ++s)
     {
+#if !CCOIL_FP64_STAGE
+        if (active)
+            integrateSegment64<FIELD, LANES>(blob + segs[s].offset, px, py, pz, lane, acc);
+#else
         const int stage = s % kSegmentStages;
         const unsigned parity = (unsigned)((s / kSegmentStages) & 1);
         bool ok = mbarWait(&bars[stage], parity);
@@ -149,6 +166,7 @@ __global__ void __launch_bounds__(128) fieldsKernel64(const unsigned char *__res
         if (threadIdx.x == 0 && s + kSegmentStages < nseg)
             stageSegment(smem + stage * kSegmentBytes, blob + segs[s + kSegmentStages].offset,
                          (unsigned)segs[s + kSegmentStages].bytes, &bars[stage]);
+#endif
     }
 
     // combine the LANES partial sums of each point (fixed order -> reproducible)
@@ -176,8 +194,9 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     long long blocks = (L.npts + ppb - 1) / ppb;
     if (blocks > 2147483647LL)
         return cudaErrorInvalidConfiguration;
-    size_t smem = (size_t)kSegmentStages * kSegmentBytes;
     const bool fp32 = L.precision == CCOIL_PRECISION_FP32_COMPENSATED;
+    const bool staged = fp32 ? CCOIL_FP32_STAGE : CCOIL_FP64_STAGE;
+    const size_t smem = staged ? (size_t)kSegmentStages * kSegmentBytes : 0;
     NearPair *work = reinterpret_cast<NearPair *>(L.d_work);
     switch (L.lanes)
     {
@@ -254,11 +273,10 @@ int launchBatch(const BatchLaunch &B, void *stream)
 int batchBlocksPerSM(int precision)
 {
     int n = 0;
-    const size_t smem = (size_t)kSegmentStages * kSegmentBytes;
     cudaError_t e = precision == CCOIL_PRECISION_FP64
-                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<CCOIL_PRECISION_FP64>, 128, smem)
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batchKernel<CCOIL_PRECISION_FP64>, 128, 0)
                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                              &n, batchKernel<CCOIL_PRECISION_FP32_COMPENSATED>, 128, smem);
+                              &n, batchKernel<CCOIL_PRECISION_FP32_COMPENSATED>, 128, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 

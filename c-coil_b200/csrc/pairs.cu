@@ -575,13 +575,21 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     return true;
 }
 
+// Stream-ordered temporary (cudaMallocAsync / cudaFreeAsync from the device's
+// default pool): no device-wide synchronisation per call
 struct DevBuf
 {
     void *p = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t alloc(size_t bytes, cudaStream_t s)
+    {
+        st = s;
+        return cudaMallocAsync(&p, bytes, s);
+    }
     ~DevBuf()
     {
         if (p)
-            cudaFree(p);
+            cudaFreeAsync(p, st);
     }
 };
 } // namespace
@@ -637,21 +645,21 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
             return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
     }
     DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ;
-    cudaError_t e = cudaMalloc(&dBlob.p, blob.size());
+    cudaError_t e = dBlob.alloc(blob.size(), st);
     if (e == cudaSuccess)
-        e = cudaMalloc(&dOff.p, sizeof(long long) * offsets.size());
+        e = dOff.alloc(sizeof(long long) * offsets.size(), st);
     if (e == cudaSuccess)
-        e = cudaMalloc(&dZ.p, sizeof(unsigned long long));
+        e = dZ.alloc(sizeof(unsigned long long), st);
     if (e == cudaSuccess && memory == CCOIL_MEMORY_HOST)
     {
-        e = cudaMalloc(&dSec.p, sizeof(double) * 5 * count);
+        e = dSec.alloc(sizeof(double) * 5 * count, st);
         if (e == cudaSuccess && primary_poses)
-            e = cudaMalloc(&dPrim.p, sizeof(double) * 5 * count);
+            e = dPrim.alloc(sizeof(double) * 5 * count, st);
         if (e == cudaSuccess)
-            e = cudaMalloc(&dOut.p, sizeof(double) * width * count);
+            e = dOut.alloc(sizeof(double) * width * count, st);
     }
     if (e != cudaSuccess)
-        return cudaFail(e, "cudaMalloc");
+        return cudaFail(e, "cudaMallocAsync");
     e = cudaMemcpyAsync(dBlob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dOff.p, offsets.data(), sizeof(long long) * offsets.size(), cudaMemcpyHostToDevice, st);
@@ -704,7 +712,7 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     unsigned long long zcount = 0;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&zcount, zc, sizeof(zcount), cudaMemcpyDeviceToHost, st);
-    // the temporary device buffers are released on return: wait for the kernel
+    // the call is synchronous, as the reference's: host outputs and the z-axis count
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
     if (e != cudaSuccess)

@@ -4,6 +4,9 @@
 //
 // Each thread runs 8 independent dependency chains so the pipes, not the
 // latency, limit the rate; the grid is 4 CTAs of 256 threads per SM.
+// ccoil_measure_op_rates adds the rates of the FP64 divide, square root and
+// logarithm the FP64 field kernels use, which expand to several FP64-pipe
+// instructions each; the roofline model charges them at these measured rates.
 #include "ccoil_internal.h"
 
 #include <cuda_runtime.h>
@@ -72,6 +75,36 @@ __global__ void mufuKernel(float *sink, int iters)
         sink[0] = s;
 }
 
+// One double-precision operation per chain and iteration, followed by one add
+// that keeps the values in range (each iteration is a contraction with a fixed
+// point near 1.6 - 3.2); the add's FP64 pipe slot is removed from the rate.
+// OP 0: __ddiv_rn(1, v), 1: __dsqrt_rn(v), 2: log(v)
+template <int OP>
+__global__ void op64Kernel(double *sink, int iters)
+{
+    double v[kChains];
+#pragma unroll
+    for (int i = 0; i < kChains; ++i)
+        v[i] = 1.5 + threadIdx.x * 1e-4 + i * 1e-2;
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int i = 0; i < kChains; ++i)
+        {
+            if (OP == 0)
+                v[i] = __dadd_rn(__ddiv_rn(1.0, v[i]), 1.0);
+            else if (OP == 1)
+                v[i] = __dadd_rn(__dsqrt_rn(v[i]), 1.0);
+            else
+                v[i] = __dadd_rn(log(v[i]), 2.0);
+        }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < kChains; ++i)
+        s += v[i];
+    if (s == 1.2345)
+        sink[0] = s;
+}
+
 template <typename Launch>
 float timeIt(Launch launch)
 {
@@ -93,6 +126,49 @@ float timeIt(Launch launch)
 } // namespace ccoil
 
 using namespace ccoil;
+
+extern "C" int ccoil_measure_op_rates(double *rates, int count)
+{
+    if (!rates || count < 6)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "rates needs 6 entries");
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_NO_DEVICE, cudaGetErrorString(e));
+    void *sink = nullptr;
+    e = cudaMalloc(&sink, 64);
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_OUT_OF_MEMORY, cudaGetErrorString(e));
+    const int blocks = sms * 4, threads = 256;
+    const double lanes = double(blocks) * threads * kChains;
+    const int it64 = 4096, it32 = 16384, itMufu = 4096, itOp = 512;
+    float ms64 = timeIt([&] { fma64Kernel<<<blocks, threads>>>((double *)sink, it64, 0.999999, 1e-7); });
+    float ms32 = timeIt([&] { fma32Kernel<<<blocks, threads>>>((float *)sink, it32, 0.999999f, 1e-7f); });
+    float msMu = timeIt([&] { mufuKernel<<<blocks, threads>>>((float *)sink, itMufu); });
+    float msDiv = timeIt([&] { op64Kernel<0><<<blocks, threads>>>((double *)sink, itOp); });
+    float msSqrt = timeIt([&] { op64Kernel<1><<<blocks, threads>>>((double *)sink, itOp); });
+    float msLog = timeIt([&] { op64Kernel<2><<<blocks, threads>>>((double *)sink, itOp); });
+    e = cudaGetLastError();
+    cudaFree(sink);
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+    const double dfma = lanes * it64 / (ms64 * 1e-3);  // FP64 pipe instructions per second
+    const double opLanes = lanes * itOp;
+    const double addSeconds = opLanes / dfma;           // the loop's own add per iteration
+    auto rate = [&](float ms) {
+        const double t = ms * 1e-3 - addSeconds;
+        return t > 0.0 ? opLanes / t : 0.0;
+    };
+    rates[0] = dfma;
+    rates[1] = rate(msDiv);
+    rates[2] = rate(msSqrt);
+    rates[3] = rate(msLog);
+    rates[4] = lanes * it32 / (ms32 * 1e-3);             // FP32 FMA instructions per second
+    rates[5] = lanes * itMufu / (msMu * 1e-3);           // MUFU rsqrt per second
+    return CCOIL_OK;
+}
 
 extern "C" int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops, double *mufu_tops)
 {

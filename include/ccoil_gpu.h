@@ -290,6 +290,14 @@ int ccoil_fields_fp32c_static(const ccoil_coil_t *coils, int coil_count, const d
  * root (tera-ops/s).  Used as roofline denominators. */
 int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops, double *mufu_tops);
 
+/* Diagnostic with no counterpart in the reference: measured rates (operations
+ * per second, whole device) of rates[0] FP64-pipe instructions (FMA),
+ * rates[1] __ddiv_rn, rates[2] __dsqrt_rn, rates[3] double log,
+ * rates[4] FP32 FMA instructions, rates[5] MUFU reciprocal square root.
+ * count must be >= 6.  The roofline model of the field kernels charges each
+ * divide, square root and logarithm rates[0] / rates[k] FP64-pipe slots. */
+int ccoil_measure_op_rates(double *rates, int count);
+
 #ifdef __cplusplus
 }
 #endif
