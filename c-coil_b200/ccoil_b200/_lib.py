@@ -47,6 +47,7 @@ class PoseStruct(ctypes.Structure):
 
 
 PAIR_MUTUAL_INDUCTANCE, PAIR_FORCE_TORQUE, PAIR_MUTUAL_INDUCTANCE_GRADIENT = 0, 1, 2
+PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT = 3
 
 
 class CCoilError(RuntimeError):

@@ -10,6 +10,14 @@ parameters (or passed explicitly), so the quadrature is a smooth function of
 the parameters.  Forward: FP64 kernel for float64 points, FP32-compensated for
 float32 points; backward: the FP64 adjoint in both cases.
 
+    M = mutual_inductance(geom1, geom2, poses1, poses2)   # (n,)
+    geom = [R, a, b, N] per coil (tensors), poses = (n, 5) [x, y, z, y_angle, z_angle]
+
+differentiates the mutual inductance of n arrangements of one primary and one
+secondary with respect to both coils' R, a, b, N and every arrangement's
+poses, through the pair kernel's exact parameter gradient (FP64; node counts
+fixed at the given geometry).
+
 `mutual_inductance_position_gradient` is the exact derivative of the mutual
 inductance quadrature with respect to the secondary's position (the pair
 kernel differentiates the primary's A at every secondary node).  Physically
@@ -103,3 +111,68 @@ def mutual_inductance_position_gradient_from_force(primary, secondary, precision
     """F / (I1 I2) with F the force on the secondary (src/Coil/ForceAndTorque/CalculateForceGeneral.cxx)."""
     F, _ = Coil.compute_force_torque(primary, secondary, precision_factor or PrecisionFactor())
     return F / (primary.get_current() * secondary.get_current())
+
+
+def pair_precisions_for(geom1, geom2, precision_factor=5.0):
+    """CPU pair PrecisionArguments (primary, secondary) of two coil geometries [R, a, b, N]."""
+    g1 = [float(v) for v in geom1]
+    g2 = [float(v) for v in geom2]
+    c1 = Coil(g1[0], g1[1], g1[2], int(round(g1[3])), 1.0)
+    c2 = Coil(g2[0], g2[1], g2[2], int(round(g2[3])), 1.0)
+    return Coil._pair_args(c1, c2, _factor(precision_factor))
+
+
+def _pair_structs(g1, g2, pp, sp):
+    zero = (ctypes.c_double * 3)(0.0, 0.0, 0.0)
+    s1, s2 = _lib.CoilStruct(), _lib.CoilStruct()
+    check(lib().ccoil_coil_init(g1[0], g1[1], g1[2], 1, 1.0, 0.0, zero, 0.0, 0.0, 5.0, 0, ctypes.byref(s1)))
+    check(lib().ccoil_coil_init(g2[0], g2[1], g2[2], 1, 1.0, 0.0, zero, 0.0, 0.0, 5.0, 0, ctypes.byref(s2)))
+    # turns enter M as N1 N2: run with N = 1 and scale, so non-integer N stay differentiable
+    s1.precision = pp.to_struct()
+    s2.precision = sp.to_struct()
+    return s1, s2
+
+
+class _MutualInductance(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, geom1, geom2, poses1, poses2, precisions):
+        from .coil import _pair_arrangements
+        g1 = geom1.detach().to("cpu", torch.float64).numpy()
+        g2 = geom2.detach().to("cpu", torch.float64).numpy()
+        p1 = np.ascontiguousarray(poses1.detach().to("cpu", torch.float64).numpy())
+        p2 = np.ascontiguousarray(poses2.detach().to("cpu", torch.float64).numpy())
+        if p1.shape != p2.shape or p1.ndim != 2 or p1.shape[1] != 5:
+            raise ValueError("poses must be (n, 5) arrays of equal shape")
+        pp, sp = precisions
+        s1, s2 = _pair_structs(g1, g2, pp, sp)
+        out, _ = _pair_arrangements([s1], s2, [sp.to_struct()], p1, p2,
+                                    _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT)
+        out = out * (g1[3] * g2[3])
+        ctx.out = out
+        ctx.turns = (g1[3], g2[3])
+        ctx.devices = (geom1.device, geom2.device, poses1.device, poses2.device)
+        ctx.dtypes = (geom1.dtype, geom2.dtype, poses1.dtype, poses2.dtype)
+        return torch.from_numpy(out[:, 0].copy()).to(poses2.device, poses2.dtype)
+
+    @staticmethod
+    def backward(ctx, grad_m):
+        out = ctx.out
+        n1, n2 = ctx.turns
+        g = grad_m.detach().to("cpu", torch.float64).numpy()
+        M = out[:, 0]
+        d1 = np.array([g @ out[:, 1], g @ out[:, 2], g @ out[:, 3], g @ M / n1])
+        d2 = np.array([g @ out[:, 6], g @ out[:, 7], g @ out[:, 8], g @ M / n2])
+        dp2 = np.concatenate([out[:, 9:12], out[:, 12:14]], axis=1) * g[:, None]
+        dp1 = np.concatenate([-out[:, 9:12], out[:, 4:6]], axis=1) * g[:, None]
+        res = [torch.from_numpy(v).to(dev, dt) for v, dev, dt in zip((d1, d2, dp1, dp2), ctx.devices, ctx.dtypes)]
+        return res[0], res[1], res[2], res[3], None
+
+
+def mutual_inductance(geom1, geom2, poses1, poses2, precisions=None, precision_factor=5.0):
+    """Differentiable mutual inductance of n arrangements: geom = [R, a, b, N] per coil, poses (n, 5)
+    = [x, y, z, y_angle, z_angle] per arrangement (primary 1, secondary 2).  Gradients flow to
+    both geometries and both pose arrays."""
+    if precisions is None:
+        precisions = pair_precisions_for(geom1.detach().cpu().numpy(), geom2.detach().cpu().numpy(),
+                                         precision_factor)
+    return _MutualInductance.apply(geom1, geom2, poses1, poses2, tuple(precisions))

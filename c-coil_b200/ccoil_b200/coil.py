@@ -209,7 +209,7 @@ def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, seco
     """Runs ccoil_pair_arrangements; returns (values, number of exact z-axis arrangements)."""
     n = len(secondary_poses)
     width = {_lib.PAIR_MUTUAL_INDUCTANCE: 1, _lib.PAIR_FORCE_TORQUE: 6,
-             _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT: 3}[quantity]
+             _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT: 3, _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT: 14}[quantity]
     out = np.zeros((n, width))
     prim = (_lib.CoilStruct * max(len(primaries), 1))(*primaries)
     secp = (_lib.PrecisionArgsStruct * max(len(sec_precisions), 1))(*sec_precisions)
@@ -384,6 +384,19 @@ class Coil:
                                   primary_z_angles, secondary_y_angles, secondary_z_angles,
                                   precision_factor or PrecisionFactor(), compute_method,
                                   _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT)
+
+    @staticmethod
+    def compute_all_mutual_inductance_parameter_gradient_arrangements(
+            primary, secondary, primary_positions, secondary_positions, primary_y_angles, primary_z_angles,
+            secondary_y_angles, secondary_z_angles, precision_factor=None, compute_method=ComputeMethod.GPU):
+        """M and its exact derivatives with respect to both coils' parameters per arrangement, (n, 14):
+        M, dM/d(R1, a1, b1, y_angle1, z_angle1, R2, a2, b2, x2, y2, z2, y_angle2, z_angle2) (no
+        counterpart in the reference).  The primary's position gradient is -dM/d(x2, y2, z2) and
+        dM/dN = M / N for either coil."""
+        return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
+                                  primary_z_angles, secondary_y_angles, secondary_z_angles,
+                                  precision_factor or PrecisionFactor(), compute_method,
+                                  _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT)
 
     @staticmethod
     def compute_all_force_torque_arrangements(primary, secondary, primary_positions, secondary_positions,

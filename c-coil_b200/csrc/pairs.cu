@@ -47,6 +47,10 @@ struct alignas(16) PairHeader
     double prim_z_angle;
     int s_nl, s_nt, s_na, s_ablocks;  // secondary node counts and angular blocks
     int off_sl, off_st, off_sa, pad2; // secondary tables (16-byte units from the header)
+    // parameter-gradient tables (16-byte units; 0 when absent): d(node position)/d(dimension)
+    // of the primary's thickness and length nodes and of the secondary's length and
+    // thickness nodes, i.e. the nodes' positions on [0, 1] (thickness) or [-1/2, 1/2] (length)
+    int off_tu, off_lu, off_slu, off_stu;
 };
 static_assert(sizeof(PairHeader) % 16 == 0, "pair header alignment");
 
@@ -176,6 +180,107 @@ __device__ __forceinline__ void segmentAGrad64(const SegmentHeader &h, const dou
     }
 }
 
+// Derivatives of the primary's A_phi(r, z) at one point (coil frame) for the
+// parameter gradient, given its value a: with respect to r and z (for the
+// Jacobian) and to the primary's inner radius R, thickness a and length b.
+// With the current density N I / (a b) folded into the node weights, the
+// thickness integral (a / 2) sum w_i f(r'_i) makes the weights independent of
+// a, so d/dR = sum w_i df/dr', d/da = sum w_i u_i df/dr' (u_i = dr'_i/da), and
+// for the fast method d/db = -a/b + the derivative of the length limits
+// (top, bot = z +- b/2); for the slow method d/db moves the length nodes.
+//   fast node  f = r' c V,  V = asinh(top/rho) - asinh(bot/rho)
+//              df/dr' = c V - r' c (r' - r c)(top g1 - bot g2) / rho^2,  dV/db = (g1 + g2) / 2
+//   slow node  f = r' c g,  g = D^-1/2
+//              df/dr' = c g - r' c (r' - r c) g^3,  df/dzl = -r' c zl g^3
+// out: {dA/dr, dA/dz, dA/dR, dA/da, dA/db}
+__device__ __noinline__ void segmentAParams64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                              const double2 *pt, const double2 *tu, const double2 *lu,
+                                              const Frame &f, double a, double *out)
+{
+    const double r = f.r;
+    double Ar = 0.0, Az = 0.0, dR = 0.0, dA = 0.0, dB = 0.0;
+    if (h.fast)
+    {
+        const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            const double p = t.x;
+            double sr = 0.0, sz = 0.0, sp = 0.0, sb = 0.0;
+            for (int k = 0; k < h.n_phi; ++k)
+            {
+                const double2 q = pt[k];
+                const double c = q.x;
+                const double rho2 = p * p + r * r - 2.0 * p * r * c;
+                const double g1 = rsqrt(rho2 + top * top), g2 = rsqrt(rho2 + bot * bot);
+                const double irho = rsqrt(rho2);
+                const double V = asinh(top * irho) - asinh(bot * irho);
+                const double tg = top * g1 - bot * g2;
+                sz += q.y * c * (g1 - g2);
+                sr -= q.y * c * (r - p * c) * tg / rho2;
+                sp += q.y * c * (V - p * (p - r * c) * tg / rho2);
+                sb += q.y * c * 0.5 * (g1 + g2);
+            }
+            Ar += t.y * p * sr;
+            Az += t.y * p * sz;
+            dR += t.y * sp;
+            dA += t.y * tu[j].x * sp;
+            dB += t.y * p * sb;
+        }
+        dB -= a / (2.0 * h.half_length);
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            const double2 l = lt[i];
+            const double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double p = t.x;
+                double sr = 0.0, sz = 0.0, sp = 0.0;
+                for (int k = 0; k < h.n_phi; ++k)
+                {
+                    const double2 q = pt[k];
+                    const double c = q.x;
+                    const double D = p * p + r * r - 2.0 * p * r * c + zl * zl;
+                    const double g = rsqrt(D), g3 = g * g * g;
+                    sz -= q.y * c * zl * g3;
+                    sr -= q.y * c * (r - p * c) * g3;
+                    sp += q.y * (c * g - p * c * (p - r * c) * g3);
+                }
+                const double w = l.y * t.y;
+                Ar += w * p * sr;
+                Az += w * p * sz;
+                dR += w * sp;
+                dA += w * tu[j].x * sp;
+                dB += w * lu[i].x * p * sz;
+            }
+        }
+    }
+    out[0] = Ar;
+    out[1] = Az;
+    out[2] = dR;
+    out[3] = dA;
+    out[4] = dB;
+}
+
+// d T / d(y axis angle) and d T / d(z axis angle) of poseFromAngles' transform
+__device__ __forceinline__ void transformDerivatives(double yA, double zA, double *dTy, double *dTz)
+{
+    double sY, cY, sZ, cZ;
+    sincos(yA, &sY, &cY);
+    sincos(zA, &sZ, &cZ);
+    dTy[0] = -cZ * cZ * sY; dTy[1] = sZ * cZ * sY;  dTy[2] = cZ * cY;
+    dTy[3] = -sZ * cZ * sY; dTy[4] = sZ * sZ * sY;  dTy[5] = sZ * cY;
+    dTy[6] = -cY * cZ;      dTy[7] = cY * sZ;       dTy[8] = -sY;
+    const double c2 = cZ * cZ - sZ * sZ, s2 = 2.0 * sZ * cZ;
+    dTz[0] = -s2 * (cY + 1.0); dTz[1] = -c2 * (cY + 1.0); dTz[2] = -sZ * sY;
+    dTz[3] = c2 * (cY + 1.0);  dTz[4] = -s2 * (1.0 + cY); dTz[5] = cZ * sY;
+    dTz[6] = sY * sZ;          dTz[7] = sY * cZ;          dTz[8] = 0.0;
+}
+
 #ifndef CCOIL_PAIR_MIN_BLOCKS
 #define CCOIL_PAIR_MIN_BLOCKS 6
 #endif
@@ -193,6 +298,7 @@ struct WarpPose
     double sp[3];                // secondary centre
     double sA, cA, sB, cB;       // sin / cos of the secondary's y and z axis angles
     double offset, ablk;         // secondary azimuth offset and angular block size
+    double dTy[9], dTz[9];       // d(primary transform)/d(y, z axis angle) (parameter gradient only)
 };
 
 // FP64 primary quadrature at one secondary node, out of line for the FP32
@@ -259,7 +365,7 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
             dst[i] = src[i];
         __syncthreads();
     }
-    constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : 3;
+    constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : QTY == 2 ? 3 : 14;
     const int lane = threadIdx.x % 32;
     volatile WarpPose &S = warpPoses[threadIdx.x / 32];
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
@@ -333,6 +439,16 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                 S.cB = cB;
                 S.offset = offset;
                 S.ablk = (improved ? kPi : 2 * kPi) / ph.s_ablocks;
+                if (QTY == 3)
+                {
+                    double dTy[9], dTz[9];
+                    transformDerivatives(ppose[3], ppose[4], dTy, dTz);
+                    for (int i = 0; i < 9; ++i)
+                    {
+                        S.dTy[i] = dTy[i];
+                        S.dTz[i] = dTz[i];
+                    }
+                }
             }
             __syncwarp();
             const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
@@ -376,6 +492,85 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                                  Az = S.T[6] * vx + S.T[7] * vy;
                     if (valid)
                         part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
+                }
+                else if (QTY == 3)
+                {
+                    // parameter gradient: per secondary node, the derivative of
+                    // w (A(q) . t) with respect to every coil parameter
+                    const double2 *tu = reinterpret_cast<const double2 *>(base) + ph.off_tu;
+                    const double2 *lu = reinterpret_cast<const double2 *>(base) + ph.off_lu;
+                    const double ul = (reinterpret_cast<const double2 *>(base) + ph.off_slu)[l].x;
+                    const double ut = (reinterpret_cast<const double2 *>(base) + ph.off_stu)[t].x;
+                    const double av = pairA64(h, tt, lt, pt, f);
+                    double d[5];
+                    segmentAParams64(h, tt, lt, pt, tu, lu, f, av, d);
+                    const double ar = d[0], az = d[1];
+                    const double c = f.cphi, s_ = f.sphi;
+                    const double ao = f.r > 0.0 ? av / f.r : ar;
+                    const double J[9] = {s_ * c * (ao - ar), -s_ * s_ * ar - c * c * ao, -s_ * az,
+                                         c * c * ar + s_ * s_ * ao, s_ * c * (ar - ao), c * az,
+                                         0.0, 0.0, 0.0};
+                    double e[3], u[3], v[3], gp[3];
+                    for (int i = 0; i < 3; ++i)
+                        e[i] = -S.T[3 * i] * s_ + S.T[3 * i + 1] * c;                      // T (-sin, cos, 0)
+                    for (int i = 0; i < 3; ++i)
+                        u[i] = S.T[i] * tan[0] + S.T[3 + i] * tan[1] + S.T[6 + i] * tan[2];  // T^T t
+                    for (int i = 0; i < 3; ++i)
+                        v[i] = J[i] * u[0] + J[3 + i] * u[1] + J[6 + i] * u[2];           // J^T u
+                    for (int i = 0; i < 3; ++i)
+                        gp[i] = S.T[3 * i] * v[0] + S.T[3 * i + 1] * v[1] + S.T[3 * i + 2] * v[2];
+                    const double et = e[0] * tan[0] + e[1] * tan[1] + e[2] * tan[2];
+                    double g[14];
+                    g[0] = av * et;
+                    g[1] = d[2] * et;
+                    g[2] = d[3] * et;
+                    g[3] = d[4] * et;
+                    // primary orientation: (dT A_loc) . t + (J_loc dT^T (q - c)) . (T^T t)
+                    const double aloc[2] = {-s_ * av, c * av};
+                    const double dv[3] = {q[0] - S.pos[0], q[1] - S.pos[1], q[2] - S.pos[2]};
+                    for (int k = 0; k < 2; ++k)
+                    {
+                        double dT[9];
+                        for (int i = 0; i < 9; ++i)
+                            dT[i] = k == 0 ? S.dTy[i] : S.dTz[i];
+                        double y[3], gk = 0.0;
+                        for (int j = 0; j < 3; ++j)
+                            y[j] = dT[j] * dv[0] + dT[3 + j] * dv[1] + dT[6 + j] * dv[2];
+                        for (int i = 0; i < 3; ++i)
+                        {
+                            gk += (dT[3 * i] * aloc[0] + dT[3 * i + 1] * aloc[1]) * tan[i];
+                            gk += (J[3 * i] * y[0] + J[3 * i + 1] * y[1] + J[3 * i + 2] * y[2]) * u[i];
+                        }
+                        g[4 + k] = gk;
+                    }
+                    // secondary inner radius, thickness, length (node positions; the
+                    // weight is proportional to the ring radius)
+                    const double axis[3] = {sA * cB, sA * sB, cA};
+                    g[6] = av * et / R.x + ringP[0] * gp[0] + ringP[1] * gp[1] + ringP[2] * gp[2];
+                    g[7] = ut * g[6];
+                    g[8] = ul * (axis[0] * gp[0] + axis[1] * gp[1] + axis[2] * gp[2]);
+                    g[9] = gp[0];
+                    g[10] = gp[1];
+                    g[11] = gp[2];
+                    // secondary orientation: node position and tangent move
+                    const double A_[3] = {av * e[0], av * e[1], av * e[2]};
+                    const double dE1A[3] = {-cB * sA, -sB * sA, -cA}, dAxA[3] = {cA * cB, cA * sB, -sA};
+                    const double dE1B[3] = {-sB * cA, cB * cA, 0.0}, dE2B[3] = {-cB, -sB, 0.0},
+                                 dAxB[3] = {-sA * sB, sA * cB, 0.0};
+                    double gA = 0.0, gB = 0.0;
+                    for (int i = 0; i < 3; ++i)
+                    {
+                        const double dqA = L.x * dAxA[i] + R.x * cP * dE1A[i], dtA = -sP * dE1A[i];
+                        const double dqB = L.x * dAxB[i] + R.x * (cP * dE1B[i] + sP * dE2B[i]),
+                                     dtB = -sP * dE1B[i] + cP * dE2B[i];
+                        gA += dqA * gp[i] + A_[i] * dtA;
+                        gB += dqB * gp[i] + A_[i] * dtB;
+                    }
+                    g[12] = gA;
+                    g[13] = gB;
+                    if (valid)
+                        for (int i = 0; i < 14; ++i)
+                            part[i] += g[i] * w;
                 }
                 else if (QTY == 2)
                 {
@@ -457,7 +652,7 @@ void put(std::vector<unsigned char> &blob, const void *p, size_t n)
 // (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
 // cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
 bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa, bool fp32,
-               std::vector<unsigned char> &blob, std::string &err)
+               bool units, std::vector<unsigned char> &blob, std::string &err)
 {
     if (!validArgs(pp) || !validArgs(spa))
     {
@@ -558,6 +753,34 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
         h.off_f32 = ph.off_sa + 2 * ph.s_na;
         setNearBox(prim, h);
     }
+    // parameter-gradient tables: each node's position per unit of its layer's
+    // dimension, {u, 0} (thickness on [0, 1], length on [-1/2, 1/2])
+    std::vector<double> tu_, lu_, slu_, stu_;
+    if (units)
+    {
+        auto thicknessUnits = [](const PrecisionArgs &a, std::vector<double> &o) {
+            const double *x = legendreNodes(a.thickness_increments);
+            for (int b = 0; b < a.thickness_blocks; ++b)
+                for (int i = 0; i < a.thickness_increments; ++i)
+                    o.insert(o.end(), {((b + 0.5) + 0.5 * x[i]) / a.thickness_blocks, 0.0});
+        };
+        auto lengthUnits = [](const PrecisionArgs &a, std::vector<double> &o) {
+            const double *x = legendreNodes(a.length_increments);
+            for (int b = 0; b < a.length_blocks; ++b)
+                for (int i = 0; i < a.length_increments; ++i)
+                    o.insert(o.end(), {-0.5 + ((b + 0.5) + 0.5 * x[i]) / a.length_blocks, 0.0});
+        };
+        thicknessUnits(pp, tu_);
+        if (!fast)
+            lengthUnits(pp, lu_);
+        lengthUnits(spa, slu_);
+        thicknessUnits(spa, stu_);
+        const int base16 = ph.off_sa + 2 * ph.s_na + (int)p32.size();
+        ph.off_tu = base16;
+        ph.off_lu = ph.off_tu + (int)tu_.size() / 2;
+        ph.off_slu = ph.off_lu + (int)lu_.size() / 2;
+        ph.off_stu = ph.off_slu + (int)slu_.size() / 2;
+    }
     const double blocks = double(spa.length_blocks) * spa.thickness_blocks * spa.angular_blocks;
     ph.m_factor = 2 * kPi * sec.num_turns / prim.current / blocks;
     ph.f_factor = 2 * kPi * (sec.current * sec.num_turns) / blocks;
@@ -571,6 +794,10 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     put(blob, st_.data(), sizeof(double) * st_.size());
     put(blob, sa_.data(), sizeof(SecAngular) * sa_.size());
     put(blob, p32.data(), sizeof(PhiNode32) * p32.size());
+    put(blob, tu_.data(), sizeof(double) * tu_.size());
+    put(blob, lu_.data(), sizeof(double) * lu_.size());
+    put(blob, slu_.data(), sizeof(double) * slu_.size());
+    put(blob, stu_.data(), sizeof(double) * stu_.size());
     (void)start;
     return true;
 }
@@ -612,18 +839,25 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     if (primary_poses && primary_count != 1)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "per-arrangement primary poses need exactly one primary");
     if (quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE && quantity != CCOIL_PAIR_FORCE_TORQUE &&
-        quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
+        quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT && quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown pair quantity");
+    if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT && count > 0 && (primary_count != 1 || !primary_poses))
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT,
+                           "the parameter gradient needs exactly one primary with per-arrangement poses");
     if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown precision mode");
-    if (precision == CCOIL_PRECISION_FP32_COMPENSATED && quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
-        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "the mutual-inductance gradient is evaluated in FP64 only");
+    if (precision == CCOIL_PRECISION_FP32_COMPENSATED && (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT ||
+                                                          quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT))
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "the mutual-inductance gradients are evaluated in FP64 only");
     const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
     if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
     if (z_axis_count)
         *z_axis_count = 0;
-    const int width = quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE ? 1 : quantity == CCOIL_PAIR_FORCE_TORQUE ? 6 : 3;
+    const int width = quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE            ? 1
+                      : quantity == CCOIL_PAIR_FORCE_TORQUE               ? 6
+                      : quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT ? 3
+                                                                          : 14;
     if (count == 0)
         return CCOIL_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -641,7 +875,8 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     for (int j = 0; j < primary_count; ++j)
     {
         offsets.push_back((long long)blob.size());
-        if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], fp32, blob, err))
+        if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], fp32,
+                       quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, blob, err))
             return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
     }
     DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ;
@@ -701,8 +936,11 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
         pairKernel64<1, true><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
                                                                     stagedBytes);
-    else
+    else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
         pairKernel64<2, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
+                                                                     stagedBytes);
+    else
+        pairKernel64<3, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
                                                                      stagedBytes);
     e = cudaGetLastError();
     if (e != cudaSuccess)

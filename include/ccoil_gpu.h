@@ -171,9 +171,19 @@ typedef enum ccoil_pair_quantity
 {
     CCOIL_PAIR_MUTUAL_INDUCTANCE = 0, /* M, one double per arrangement */
     CCOIL_PAIR_FORCE_TORQUE = 1,      /* Fx Fy Fz Tx Ty Tz on the secondary, six doubles per arrangement */
-    CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT = 2 /* dM/d(secondary position): the exact derivative of the M
-                                                 quadrature (adjoint of M; no counterpart in the reference),
-                                                 three doubles per arrangement */
+    CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT = 2, /* dM/d(secondary position): the exact derivative of the M
+                                                  quadrature (adjoint of M; no counterpart in the reference),
+                                                  three doubles per arrangement */
+    CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT = 3 /* M and its exact derivatives with respect to both
+                                                           coils' parameters (no counterpart in the reference),
+                                                           14 doubles per arrangement:
+                                                           M, dM/dR1, dM/da1, dM/db1, dM/dyAngle1, dM/dzAngle1,
+                                                           dM/dR2, dM/da2, dM/db2, dM/dx2, dM/dy2, dM/dz2,
+                                                           dM/dyAngle2, dM/dzAngle2 (1 = primary, 2 = secondary;
+                                                           R inner radius, a thickness, b length).  The primary's
+                                                           position gradient is -dM/d(x2, y2, z2) and
+                                                           dM/dN = M / N for either coil.  One primary with
+                                                           per-arrangement poses; FP64 only. */
 } ccoil_pair_quantity_t;
 
 /* Position and orientation of a coil (Coil::setPositionAndOrientation,

@@ -99,3 +99,100 @@ def test_mutual_inductance_position_gradient(ccoil, oracle):
             fd[k] = (m[0] - m[1]) / (2 * h)
         assert np.max(np.abs(g - fd)) <= 1e-6 * np.max(np.abs(fd)), (i, g, fd)
     assert worst_force < 1e-3, worst_force
+
+
+def _pose_rows(seed, n):
+    g = np.random.default_rng(seed)
+    p1 = np.concatenate([g.uniform(-0.05, 0.05, (n, 3)), g.uniform(0.2, 1.2, (n, 1)),
+                         g.uniform(0, 2 * np.pi, (n, 1))], axis=1)
+    off = g.normal(size=(n, 3))
+    off *= (0.25 / np.linalg.norm(off, axis=1))[:, None]
+    p2 = np.concatenate([p1[:, :3] + off, g.uniform(0.2, 1.2, (n, 1)), g.uniform(0, 2 * np.pi, (n, 1))], axis=1)
+    return p1, p2
+
+
+def _frame(y, z):
+    """[e1 e2 axis] of a coil's ring basis at axis angles (y, z), as the pair kernel builds the node cloud."""
+    sA, cA, sB, cB = np.sin(y), np.cos(y), np.sin(z), np.cos(z)
+    return np.array([[cB * cA, -sB, sA * cB], [sB * cA, cB, sA * sB], [-sA, 0.0, cA]])
+
+
+@pytest.mark.parametrize("prim_geom,skip", [((0.1, 0.05, 0.1, 200.0), ()),
+                                            ((0.1, 0.05, 0.0, 150.0), ("b1",))])
+def test_mutual_inductance_parameter_gradient(ccoil, oracle, prim_geom, skip):
+    """Adjoint of M with respect to both coils' R, a, b, N and both poses against central
+    differences (node counts fixed); RECTANGULAR (fast) and FLAT (slow method) primaries."""
+    import torch
+    from ccoil_b200.autograd import mutual_inductance, pair_precisions_for
+    n = 6
+    p1, p2 = _pose_rows(31, n)
+    g1 = np.array(prim_geom)
+    g2 = np.array([0.05, 0.02, 0.08, 100.0])
+    precs = pair_precisions_for(g1, g2, 5.0)
+    coef = np.random.default_rng(7).uniform(0.5, 1.5, n)
+
+    def loss(a, b, c, d):
+        m = mutual_inductance(torch.tensor(a), torch.tensor(b), torch.tensor(c), torch.tensor(d), precs)
+        return float((m.numpy() * coef).sum()), m
+
+    G1, G2 = torch.tensor(g1, requires_grad=True), torch.tensor(g2, requires_grad=True)
+    P1, P2 = torch.tensor(p1, requires_grad=True), torch.tensor(p2, requires_grad=True)
+    m = mutual_inductance(G1, G2, P1, P2, precs)
+    (m * torch.tensor(coef)).sum().backward()
+
+    # M itself is the arrangement kernel's M
+    prim = ccoil.Coil(g1[0], g1[1], g1[2], int(g1[3]), 1.0)
+    sec = ccoil.Coil(g2[0], g2[1], g2[2], int(g2[3]), 1.0)
+    ref_m = ccoil.Coil.compute_all_mutual_inductance_arrangements(
+        prim, sec, p1[:, :3], p2[:, :3], p1[:, 3], p1[:, 4], p2[:, 3], p2[:, 4], ccoil.PrecisionFactor(5.0))
+    assert np.max(np.abs(m.detach().numpy() - ref_m) / np.abs(ref_m)) < 1e-12
+
+    def fd(arrs, which, idx, h):
+        up = [a.copy() for a in arrs]
+        dn = [a.copy() for a in arrs]
+        up[which][idx] += h
+        dn[which][idx] -= h
+        return (loss(*up)[0] - loss(*dn)[0]) / (2 * h)
+
+    arrs = [g1, g2, p1, p2]
+    names = ("R", "a", "b", "N")
+    for which, G in ((0, G1), (1, G2)):
+        for k in range(4):
+            if "%s%d" % (names[k], which + 1) in skip:
+                continue
+            h = 1e-6 * arrs[which][k]
+            want = fd(arrs, which, k, h)
+            got = G.grad.numpy()[k]
+            print("geometry", names[k], which + 1, "rel err vs FD %.2e" % (abs(got - want) / abs(want)))
+            assert abs(got - want) <= 1e-6 * abs(want) + 1e-12 * abs(loss(*arrs)[0]) / arrs[which][k], \
+                (names[k], which + 1, got, want)
+    for which, P in ((2, P1), (3, P2)):
+        got = P.grad.numpy()
+        want = np.zeros_like(got)
+        for i in range(n):
+            for k in range(5):
+                want[i, k] = fd(arrs, which, (i, k), 1e-6 if k >= 3 else 1e-7)
+        for k, scale in ((slice(0, 3), None), (slice(3, 5), None)):
+            err = np.max(np.abs(got[:, k] - want[:, k])) / np.max(np.abs(want[:, k]))
+            print("pose", which - 1, k, "max rel err vs FD %.2e" % err)
+            assert err < 1e-6, (which, k, err, got[:, k], want[:, k])
+
+    # against the reference algorithm's force and torque on the secondary (I1 = 2, I2 = 3):
+    # F = I1 I2 dM/dc2 and T . w = I1 I2 dM/d(angle) for the rotation w that the angle turns
+    # the secondary by -- equal up to the quadrature error of PF 5
+    worst = 0.0
+    for i in range(n):
+        prow = np.array([*g1[:3], g1[3], 2.0, 0.0, *p1[i]])
+        srow = np.array([*g2[:3], g2[3], 3.0, 0.0, *p2[i]])
+        ft = oracle.force_torque(prow, srow, pf=5.0) / 6.0
+        gpos = P2.grad.numpy()[i, :3] / coef[i]
+        worst = max(worst, np.max(np.abs(gpos - ft[:3])) / np.max(np.abs(ft[:3])))
+        for k in (3, 4):
+            h = 1e-7
+            dq = (_frame(*(p2[i, 3:5] + h * np.eye(2)[k - 3])) - _frame(*(p2[i, 3:5] - h * np.eye(2)[k - 3]))) / (2 * h)
+            W = dq @ _frame(*p2[i, 3:5]).T
+            w = np.array([W[2, 1], W[0, 2], W[1, 0]])
+            tw = ft[3:] @ w
+            worst = max(worst, abs(P2.grad.numpy()[i, k] / coef[i] - tw) / np.max(np.abs(ft[3:])))
+    print("force/torque route, max rel deviation %.2e" % worst)
+    assert worst < 2e-3, worst
