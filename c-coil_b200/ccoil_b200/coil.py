@@ -205,8 +205,9 @@ def _poses(positions, y_angles, z_angles):
 
 
 def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, secondary_poses, quantity,
-                       precision_mode=PrecisionMode.FP64):
-    """Runs ccoil_pair_arrangements; returns (values, number of exact z-axis arrangements)."""
+                       precision_mode=PrecisionMode.FP64, zaxis_precisions=None):
+    """Runs ccoil_pair_arrangements (ccoil_pair_arrangements_zaxis when z-axis pair arguments
+    [primary, secondary] per primary are given); returns (values, number of exact z-axis pairs)."""
     n = len(secondary_poses)
     width = {_lib.PAIR_MUTUAL_INDUCTANCE: 1, _lib.PAIR_FORCE_TORQUE: 6,
              _lib.PAIR_MUTUAL_INDUCTANCE_GRADIENT: 3, _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT: 14}[quantity]
@@ -214,11 +215,18 @@ def _pair_arrangements(primaries, secondary, sec_precisions, primary_poses, seco
     prim = (_lib.CoilStruct * max(len(primaries), 1))(*primaries)
     secp = (_lib.PrecisionArgsStruct * max(len(sec_precisions), 1))(*sec_precisions)
     zc = ctypes.c_longlong(0)
-    check(lib().ccoil_pair_arrangements(
-        prim, len(primaries), ctypes.byref(secondary), secp,
-        None if primary_poses is None else primary_poses.ctypes.data_as(ctypes.c_void_p),
-        secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, int(precision_mode),
-        out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(zc), _lib.MEMORY_HOST, None))
+    pposes = None if primary_poses is None else primary_poses.ctypes.data_as(ctypes.c_void_p)
+    if zaxis_precisions is None:
+        check(lib().ccoil_pair_arrangements(
+            prim, len(primaries), ctypes.byref(secondary), secp, pposes,
+            secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, int(precision_mode),
+            out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(zc), _lib.MEMORY_HOST, None))
+    else:
+        zp = (_lib.PrecisionArgsStruct * max(len(zaxis_precisions), 1))(*zaxis_precisions)
+        check(lib().ccoil_pair_arrangements_zaxis(
+            prim, len(primaries), ctypes.byref(secondary), secp, zp, pposes,
+            secondary_poses.ctypes.data_as(ctypes.c_void_p), n, quantity, int(precision_mode),
+            out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(zc), _lib.MEMORY_HOST, None))
     return (out[:, 0] if width == 1 else out), zc.value
 
 
@@ -356,8 +364,14 @@ class Coil:
         spose = _poses(secondary_positions, secondary_y_angles, secondary_z_angles)
         if len(ppose) != len(spose):
             raise ValueError("Array sizes do not match!")
+        zargs = None
+        if quantity in (_lib.PAIR_MUTUAL_INDUCTANCE, _lib.PAIR_FORCE_TORQUE):
+            # coaxial arrangements take the reference CPU path's z-axis formulas and arguments
+            za = CoilPairArguments.get_appropriate_coil_pair_arguments(primary, secondary, _factor(precision_factor),
+                                                                       ComputeMethod.CPU_ST, z_axis_case=True)
+            zargs = [za.primary_precision.to_struct(), za.secondary_precision.to_struct()]
         vals, _ = _pair_arrangements([primary.struct(pp)], secondary.struct(sp), [sp.to_struct()], ppose, spose,
-                                     quantity, precision_mode)
+                                     quantity, precision_mode, zargs)
         return vals
 
     @staticmethod
@@ -507,15 +521,20 @@ class CoilGroup:
         if ComputeMethod(compute_method) != ComputeMethod.GPU:
             raise NotImplementedError("this package provides the ComputeMethod.GPU path only")
         pf = _factor(precision_factor or PrecisionFactor())
-        prims, secs = [], []
+        prims, secs, zargs = [], [], []
         for m in self.member_coils:
             if m.get_id() == secondary.get_id():
                 continue  # CoilGroup::computeMutualInductance skips the secondary (ComputeMInductance.cxx:15)
             pp, sp = Coil._pair_args(m, secondary, pf)
             prims.append(m.struct(pp))
             secs.append(sp.to_struct())
+            za = CoilPairArguments.get_appropriate_coil_pair_arguments(m, secondary, pf, ComputeMethod.CPU_ST,
+                                                                       z_axis_case=True)
+            zargs += [za.primary_precision.to_struct(), za.secondary_precision.to_struct()]
         spose = _poses(positions, y_angles, z_angles)
-        vals, _ = _pair_arrangements(prims, secondary.struct(), secs, None, spose, quantity, precision_mode)
+        vals, _ = _pair_arrangements(prims, secondary.struct(), secs, None, spose, quantity, precision_mode,
+                                     zargs if quantity in (_lib.PAIR_MUTUAL_INDUCTANCE, _lib.PAIR_FORCE_TORQUE)
+                                     else None)
         return vals
 
     def compute_all_mutual_inductance_arrangements(self, secondary, secondary_positions, secondary_y_angles,

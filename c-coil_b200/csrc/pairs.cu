@@ -299,6 +299,7 @@ struct WarpPose
     double sA, cA, sB, cB;       // sin / cos of the secondary's y and z axis angles
     double offset, ablk;         // secondary azimuth offset and angular block size
     double dTy[9], dTz[9];       // d(primary transform)/d(y, z axis angle) (parameter gradient only)
+    int skip;                    // coaxial pair left to the z-axis pass
 };
 
 // FP64 primary quadrature at one secondary node, out of line for the FP32
@@ -353,7 +354,9 @@ template <int QTY, bool FP32>
 __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
                  const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
-                 double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes)
+                 double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes,
+                 const long long *__restrict__ zOffsets, long long *__restrict__ zList,
+                 unsigned long long *__restrict__ zListCount)
 {
     extern __shared__ __align__(16) unsigned char stagedPair[];
     __shared__ WarpPose warpPoses[4];
@@ -376,6 +379,7 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
 #pragma unroll
         for (int i = 0; i < W; ++i)
             total[i] = 0.0;
+        bool hasZ = false;  // lane 0: some primary of this arrangement is left to the z-axis pass
         for (int j = 0; j < nprim; ++j)
         {
             const unsigned char *base = stagedBytes > 0 ? stagedPair : blob + primOffsets[j];
@@ -416,8 +420,12 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                     ppose[3] = ph.prim_y_angle;
                     ppose[4] = ph.prim_z_angle;
                 }
-                if (zAxisCount && zAxisCase(ppose, spose, h.inner_radius))
+                const bool isZ = zAxisCase(ppose, spose, h.inner_radius);
+                if (zAxisCount && isZ)
                     atomicAdd(zAxisCount, 1ull);
+                const bool skip = isZ && zOffsets && zOffsets[j] >= 0;
+                S.skip = skip ? 1 : 0;
+                hasZ = hasZ || skip;
                 double offset = 0.0;
                 const bool improved = QTY != 1 ? improvedCase(ppose, spose, offset) : false;
                 for (int i = 0; i < 3; ++i)
@@ -451,6 +459,8 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                 }
             }
             __syncwarp();
+            if (S.skip)
+                continue;  // warp-uniform: the z-axis pass adds this primary
             const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
             double part[W];
 #pragma unroll
@@ -638,6 +648,8 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
 #pragma unroll
             for (int i = 0; i < W; ++i)
                 out[W * a + i] = total[i];
+            if (hasZ)
+                zList[atomicAdd(zListCount, 1ull)] = a;
         }
     }
 }
@@ -648,30 +660,18 @@ void put(std::vector<unsigned char> &blob, const void *p, size_t n)
     blob.insert(blob.end(), c, c + n);
 }
 
-// Primary tables as the reference's field integrators lay them out
-// (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
-// cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
-bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa, bool fp32,
-               bool units, std::vector<unsigned char> &blob, std::string &err)
+// The primary's field tables: thickness nodes {r', constant w} with the
+// integrator's constant folded in, length nodes {z, w} (slow method) and
+// angular nodes {cos, w}, as the reference's field integrators lay them out
+// (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66).
+void primaryTables(const Coil &prim, const PrecisionArgs &pp, std::vector<double> &pt_, std::vector<double> &pl_,
+                   std::vector<double> &pa_)
 {
-    if (!validArgs(pp) || !validArgs(spa))
-    {
-        err = "pair precision arguments out of range (increments 1..100, blocks >= 1)";
-        return false;
-    }
-    if (!(prim.inner_radius > 0.0) || !(prim.thickness > 0.0) || !(prim.length > 0.0) || !(sec.inner_radius > 0.0) ||
-        !(sec.thickness > 0.0) || !(sec.length > 0.0) || prim.current == 0.0)
-    {
-        err = "coil dimensions must be positive and the primary current non-zero";
-        return false;
-    }
-    const size_t start = blob.size();
     const bool fast = prim.use_fast_method != 0;
     const double tBlock = prim.thickness / pp.thickness_blocks, aBlock = kPi / pp.angular_blocks;
     const double constant = fast ? kMuReduced * prim.current_density * tBlock * aBlock * 2 * 0.25
                                  : kMuReduced * prim.current_density * (prim.length / pp.length_blocks) * tBlock *
                                        aBlock * 2 * 0.125;
-    std::vector<double> pt_, pl_, pa_;
     const double *tx = legendreNodes(pp.thickness_increments), *tw = legendreWeights(pp.thickness_increments);
     for (int b = 0; b < pp.thickness_blocks; ++b)
         for (int i = 0; i < pp.thickness_increments; ++i)
@@ -697,6 +697,29 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
             pa_.push_back(std::cos(aBlock * (b + 0.5) + (aBlock * 0.5) * ax[i]));
             pa_.push_back(aw[i]);
         }
+}
+
+// Primary tables as the reference's field integrators lay them out
+// (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
+// cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
+bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa, bool fp32,
+               bool units, std::vector<unsigned char> &blob, std::string &err)
+{
+    if (!validArgs(pp) || !validArgs(spa))
+    {
+        err = "pair precision arguments out of range (increments 1..100, blocks >= 1)";
+        return false;
+    }
+    if (!(prim.inner_radius > 0.0) || !(prim.thickness > 0.0) || !(prim.length > 0.0) || !(sec.inner_radius > 0.0) ||
+        !(sec.thickness > 0.0) || !(sec.length > 0.0) || prim.current == 0.0)
+    {
+        err = "coil dimensions must be positive and the primary current non-zero";
+        return false;
+    }
+    const size_t start = blob.size();
+    const bool fast = prim.use_fast_method != 0;
+    std::vector<double> pt_, pl_, pa_;
+    primaryTables(prim, pp, pt_, pl_, pa_);
     // secondary cloud tables
     std::vector<double> sl_, st_;
     std::vector<SecAngular> sa_;
@@ -802,6 +825,8 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     return true;
 }
 
+#include "zaxis.cuh"
+
 // Stream-ordered temporary (cudaMallocAsync / cudaFreeAsync from the device's
 // default pool): no device-wide synchronisation per call
 struct DevBuf
@@ -826,11 +851,13 @@ int cudaFail(cudaError_t e, const char *what);
 
 using namespace ccoil;
 
-extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
-                                       const ccoil_precision_args_t *secondary_precisions,
-                                       const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
-                                       long long count, int quantity, int precision, double *out,
-                                       long long *z_axis_count, int memory, void *stream)
+extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int primary_count,
+                                             const ccoil_coil_t *secondary,
+                                             const ccoil_precision_args_t *secondary_precisions,
+                                             const ccoil_precision_args_t *zaxis_precisions,
+                                             const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
+                                             long long count, int quantity, int precision, double *out,
+                                             long long *z_axis_count, int memory, void *stream)
 {
     if (primary_count < 0 || (primary_count > 0 && (!primaries || !secondary_precisions)) || !secondary)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "null coils or negative primary_count");
@@ -879,12 +906,37 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
                        quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, blob, err))
             return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
     }
-    DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ;
+    const size_t generalBytes = blob.size();
+    // coaxial pairs: the z-axis tables of every primary (M and F/T only)
+    const bool zPass = zaxis_precisions && (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE ||
+                                            quantity == CCOIL_PAIR_FORCE_TORQUE);
+    std::vector<long long> zOffsets(primary_count, -1);
+    if (zPass)
+        for (int j = 0; j < primary_count; ++j)
+        {
+            zOffsets[j] = (long long)blob.size();
+            if (!buildZAxis(primaries[j], *secondary, zaxis_precisions[2 * j], zaxis_precisions[2 * j + 1], blob, err))
+                return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
+        }
+    DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ, dZOff, dZList, dZCount;
     cudaError_t e = dBlob.alloc(blob.size(), st);
     if (e == cudaSuccess)
         e = dOff.alloc(sizeof(long long) * offsets.size(), st);
     if (e == cudaSuccess)
         e = dZ.alloc(sizeof(unsigned long long), st);
+    if (e == cudaSuccess && zPass)
+    {
+        e = dZOff.alloc(sizeof(long long) * primary_count, st);
+        if (e == cudaSuccess)
+            e = dZList.alloc(sizeof(long long) * count, st);
+        if (e == cudaSuccess)
+            e = dZCount.alloc(sizeof(unsigned long long), st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dZOff.p, zOffsets.data(), sizeof(long long) * primary_count, cudaMemcpyHostToDevice,
+                                st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(dZCount.p, 0, sizeof(unsigned long long), st);
+    }
     if (e == cudaSuccess && memory == CCOIL_MEMORY_HOST)
     {
         e = dSec.alloc(sizeof(double) * 5 * count, st);
@@ -915,7 +967,10 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     if (e != cudaSuccess)
         return cudaFail(e, "host->device copy");
     // one primary whose tables fit: stage them in shared memory
-    const int stagedBytes = (primary_count == 1 && blob.size() <= CCOIL_PAIR_STAGE_MAX_BYTES && blob.size() % 16 == 0) ? (int)blob.size() : 0;
+    const int stagedBytes = (primary_count == 1 && generalBytes <= CCOIL_PAIR_STAGE_MAX_BYTES &&
+                             generalBytes % 16 == 0)
+                                ? (int)generalBytes
+                                : 0;
     const long long warpsNeeded = count;
     long long blocks = (warpsNeeded + 3) / 4;
     if (blocks > 148LL * 64)
@@ -924,24 +979,33 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     const auto *dB = static_cast<const unsigned char *>(dBlob.p);
     const auto *dO = static_cast<const long long *>(dOff.p);
     const size_t smem = (size_t)stagedBytes;
+    const auto *zO = static_cast<const long long *>(dZOff.p);
+    auto *zL = static_cast<long long *>(dZList.p);
+    auto *zN = static_cast<unsigned long long *>(dZCount.p);
+#define CCOIL_PAIR_LAUNCH(Q, F)                                                                                        \
+    pairKernel64<Q, F><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,       \
+                                                           stagedBytes, zO, zL, zN)
     if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE && !fp32)
-        pairKernel64<0, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                     stagedBytes);
+        CCOIL_PAIR_LAUNCH(0, false);
     else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
-        pairKernel64<0, true><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                    stagedBytes);
+        CCOIL_PAIR_LAUNCH(0, true);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE && !fp32)
-        pairKernel64<1, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                     stagedBytes);
+        CCOIL_PAIR_LAUNCH(1, false);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
-        pairKernel64<1, true><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                    stagedBytes);
+        CCOIL_PAIR_LAUNCH(1, true);
     else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
-        pairKernel64<2, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                     stagedBytes);
+        CCOIL_PAIR_LAUNCH(2, false);
     else
-        pairKernel64<3, false><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,
-                                                                     stagedBytes);
+        CCOIL_PAIR_LAUNCH(3, false);
+#undef CCOIL_PAIR_LAUNCH
+    if (zPass && cudaGetLastError() == cudaSuccess)
+    {
+        // the z-axis pass: one warp per recorded arrangement
+        if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
+            zAxisKernel<0><<<148 * 8, 128, 0, st>>>(dB, dO, zO, primary_count, primP, secP, zL, zN, o);
+        else
+            zAxisKernel<1><<<148 * 8, 128, 0, st>>>(dB, dO, zO, primary_count, primP, secP, zL, zN, o);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return cudaFail(e, "pair kernel launch");
@@ -958,4 +1022,15 @@ extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primar
     if (z_axis_count)
         *z_axis_count = (long long)zcount;
     return CCOIL_OK;
+}
+
+extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                                       const ccoil_precision_args_t *secondary_precisions,
+                                       const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
+                                       long long count, int quantity, int precision, double *out,
+                                       long long *z_axis_count, int memory, void *stream)
+{
+    return ccoil_pair_arrangements_zaxis(primaries, primary_count, secondary, secondary_precisions, nullptr,
+                                         primary_poses, secondary_poses, count, quantity, precision, out,
+                                         z_axis_count, memory, stream);
 }

@@ -213,8 +213,10 @@ typedef struct ccoil_pose
  * Calculate_force_and_torque_configurations[_group]
  * (src/Coil/CUDAKernels/CoilAcceleration.h:21-29,
  * src/CoilGroup/CUDAKernels/CoilGroupAcceleration.h:27-37).
- * Arrangements that are exact z-axis cases (Coil::isZAxisCase) are evaluated
- * with the general formula; their number is returned in *z_axis_count.
+ * (primary, arrangement) pairs that are exact z-axis cases (Coil::isZAxisCase)
+ * are evaluated here with the general formula (ccoil_pair_arrangements_zaxis
+ * uses the reference's z-axis formulas); their number is returned in
+ * *z_axis_count.
  * precision: CCOIL_PRECISION_FP64 follows the reference's double arithmetic;
  * CCOIL_PRECISION_FP32_COMPENSATED (mutual inductance and force/torque only;
  * CCOIL_ERR_NOT_SUPPORTED for the gradient) evaluates the primary's quadrature
@@ -225,6 +227,23 @@ int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, co
                             const ccoil_precision_args_t *secondary_precisions, const ccoil_pose_t *primary_poses,
                             const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
                             double *out, long long *z_axis_count, int memory, void *stream);
+
+/* The same with the reference CPU path's per-pair dispatch for coaxial pairs
+ * (Coil::computeMutualInductance, src/Coil/MInductance/ComputeMInductanceMethods.cxx:7-30;
+ * Coil::computeForceTorque, src/Coil/ForceAndTorque/ComputeForceMethods.cxx:4-23):
+ * a (primary, arrangement) pair that Coil::isZAxisCase accepts is evaluated
+ * with the z-axis formulas (src/Coil/MInductance/CalculateMInductanceZAxis.cxx:17-232,
+ * src/Coil/ForceAndTorque/CalculateForceZAxis.cxx:16-219) at the z-axis pair
+ * arguments zaxis_precisions[2j] (primary) and [2j+1] (secondary), as from
+ * ccoil_pair_arguments(..., z_axis_case = 1, ...); its force is (0, 0, Fz)
+ * and its torque zero.  Mutual inductance and force/torque only (the
+ * gradients use the general formula); zaxis_precisions == NULL is
+ * ccoil_pair_arrangements. */
+int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                                  const ccoil_precision_args_t *secondary_precisions,
+                                  const ccoil_precision_args_t *zaxis_precisions, const ccoil_pose_t *primary_poses,
+                                  const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
+                                  double *out, long long *z_axis_count, int memory, void *stream);
 
 /* ------------------------------------------------------------------------ *
  * Batched independent systems                                               *

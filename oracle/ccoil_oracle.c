@@ -895,17 +895,113 @@ static void ft_general(const OCoil *p, const OCoil *s, const OArgs *pu, const OA
     }
 }
 
-/* General-case mutual inductance with explicit pair args (args12) or, when
- * args12 is NULL, the CPU pair args at pf.  Returns 1 (and computes nothing) for
- * the coaxial case, which the reference routes to its z-axis formulas. */
+/* ------------------------------------------------------------------ */
+/* Coaxial pairs: the z-axis formulas                                   */
+/* ------------------------------------------------------------------ */
+/* Coil::calculateMutualInductanceZAxisFast (src/Coil/MInductance/CalculateMInductanceZAxis.cxx:87-232)
+ * and Coil::calculateAmpereForceZAxisFast (src/Coil/ForceAndTorque/CalculateForceZAxis.cxx:85-219):
+ * both length integrals in closed form; force != 0 selects the axial force. */
+static double zaxis_fast(const OCoil *p, const OCoil *s, double zd, const OArgs *pu, const OArgs *su, int force)
+{
+    double tb = p->a / pu->tB, ab = PI / pu->aB, rb = s->a / su->tB;
+    double constant = MI_REDUCED * p->J * s->J * tb * ab * rb * 0.125;
+    double *cs = angular_cos(pu);
+    zd -= p->pos[2];
+    double z1 = zd + s->b * 0.5 + p->b * 0.5, z2 = zd + s->b * 0.5 - p->b * 0.5;
+    double z3 = zd - s->b * 0.5 - p->b * 0.5, z4 = zd - s->b * 0.5 + p->b * 0.5;
+    double z1s = z1 * z1, z2s = z2 * z2, z3s = z3 * z3, z4s = z4 * z4;
+    double sum = 0.0;
+    for (int bR = 0; bR < su->tB; ++bR)
+    {
+        double blockR = s->R + rb * (bR + 0.5);
+        for (int iR = 0; iR < su->tI; ++iR)
+        {
+            double r = blockR + (rb * 0.5) * g_pos[su->tI - 1][iR];
+            double wR = g_wts[su->tI - 1][iR];
+            for (int bT = 0; bT < pu->tB; ++bT)
+            {
+                double blockT = p->R + tb * (bT + 0.5);
+                for (int iT = 0; iT < pu->tI; ++iT)
+                {
+                    double t = blockT + (tb * 0.5) * g_pos[pu->tI - 1][iT];
+                    double wT = g_wts[pu->tI - 1][iT];
+                    double c0 = constant * wR * wT;
+                    double A = 2.0 * t * r, B = t * t + r * r;
+                    for (int bP = 0; bP < pu->aB; ++bP)
+                        for (int iP = 0; iP < pu->aI; ++iP)
+                        {
+                            double wP = g_wts[pu->aI - 1][iP];
+                            double c = cs[bP * pu->aI + iP];
+                            double C = B - A * c, D = sqrt(C);
+                            if (!force)
+                            {
+                                double E1 = sqrt(C + z1s), E2 = sqrt(C + z2s), E3 = sqrt(C + z3s), E4 = sqrt(C + z4s);
+                                double F1 = z1 / D, F2 = z2 / D, F3 = z3 / D, F4 = z4 / D;
+                                double G1 = sqrt(F1 * F1 + 1.0), G2 = sqrt(F2 * F2 + 1.0);
+                                double G3 = sqrt(F3 * F3 + 1.0), G4 = sqrt(F4 * F4 + 1.0);
+                                double H1 = z1 * log(F1 + G1), H2 = z2 * log(F2 + G2);
+                                double H3 = z3 * log(F3 + G3), H4 = z4 * log(F4 + G4);
+                                sum += c0 * wP * A * c * (H1 - H2 + H3 - H4 - E1 + E2 - E3 + E4);
+                            }
+                            else
+                            {
+                                double E1 = z1 / D, E2 = z2 / D, E3 = z3 / D, E4 = z4 / D;
+                                double G1 = E1 + sqrt(E1 * E1 + 1.0), G2 = E2 + sqrt(E2 * E2 + 1.0);
+                                double G3 = E3 + sqrt(E3 * E3 + 1.0), G4 = E4 + sqrt(E4 * E4 + 1.0);
+                                sum += c0 * wP * A * c * log(G2 * G4 / (G1 * G3));
+                            }
+                        }
+                }
+            }
+        }
+    }
+    free(cs);
+    return force ? (-1.0) * sum * 2 * PI : sum * 2 * PI / (p->I * s->I);
+}
+
+/* Coil::calculateMutualInductanceZAxisSlow (CalculateMInductanceZAxis.cxx:17-85) and
+ * Coil::calculateAmpereForceZAxisSlow (CalculateForceZAxis.cxx:16-83): the primary's
+ * |A| (or B_x) on the secondary's (r, z) grid in the plane y = 0. */
+static double zaxis_slow(const OCoil *p, const OCoil *s, double zd, const OArgs *pu, const OArgs *su, int force)
+{
+    double lbs = s->b / su->lB, tbs = s->a / su->tB;
+    double sum = 0.0;
+    for (int bZ = 0; bZ < su->lB; ++bZ)
+        for (int bR = 0; bR < su->tB; ++bR)
+        {
+            double zBlock = (-1) * (s->b * 0.5) + lbs * (bZ + 0.5);
+            double rBlock = s->R + tbs * (bR + 0.5);
+            for (int iZ = 0; iZ < su->lI; ++iZ)
+                for (int iR = 0; iR < su->tI; ++iR)
+                {
+                    double z = zd + zBlock + (lbs * 0.5) * g_pos[su->lI - 1][iZ];
+                    double r = rBlock + (tbs * 0.5) * g_pos[su->tI - 1][iR];
+                    double w = r * 0.25 * g_wts[su->lI - 1][iZ] * g_wts[su->tI - 1][iR];
+                    double pt[3] = {r, 0.0, z}, v[3];
+                    point_field(p, pu, force ? 1 : 0, pt, v);
+                    sum += (force ? v[0] : sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])) * w;
+                }
+        }
+    sum /= (su->lB * su->tB);
+    return force ? (-1.0) * sum * 2 * PI * s->N * s->I : sum * 2 * PI * s->N / p->I;
+}
+
+static double zaxis_value(const OCoil *p, const OCoil *s, const OArgs *pu, const OArgs *su, int force)
+{
+    int fast = (p->type == RECTANGULAR || p->type == THIN) && (s->type == RECTANGULAR || s->type == THIN);
+    return fast ? zaxis_fast(p, s, s->pos[2], pu, su, force) : zaxis_slow(p, s, s->pos[2], pu, su, force);
+}
+
+/* Mutual inductance with explicit pair args (args12) or, when args12 is NULL,
+ * the CPU pair args at pf (z-axis arguments for a coaxial pair), dispatched as
+ * Coil::computeMutualInductance (src/Coil/MInductance/ComputeMInductanceMethods.cxx:7-40). */
 int oracle_mutual_inductance(const double *pc, const double *sc, double pf, const int *args12, double *out)
 {
     build_tables();
     OCoil p, s;
     make_coil(pc, &p);
     make_coil(sc, &s);
-    if (z_axis_case(&p, &s))
-        return 1;
+    int zax = z_axis_case(&p, &s);
     OArgs pu, su;
     if (args12)
     {
@@ -913,8 +1009,8 @@ int oracle_mutual_inductance(const double *pc, const double *sc, double pf, cons
         su = make_args(args12[6], args12[7], args12[8], args12[9], args12[10], args12[11]);
     }
     else
-        pair_args(&p, &s, sanitize_pf(pf), 0, 0, 0, &pu, &su);
-    *out = m_general(&p, &s, &pu, &su);
+        pair_args(&p, &s, sanitize_pf(pf), 0, zax, 0, &pu, &su);
+    *out = zax ? zaxis_value(&p, &s, &pu, &su, 0) : m_general(&p, &s, &pu, &su);
     return 0;
 }
 
@@ -924,8 +1020,7 @@ int oracle_force_torque(const double *pc, const double *sc, double pf, const int
     OCoil p, s;
     make_coil(pc, &p);
     make_coil(sc, &s);
-    if (z_axis_case(&p, &s))
-        return 1;
+    int zax = z_axis_case(&p, &s);
     OArgs pu, su;
     if (args12)
     {
@@ -933,7 +1028,15 @@ int oracle_force_torque(const double *pc, const double *sc, double pf, const int
         su = make_args(args12[6], args12[7], args12[8], args12[9], args12[10], args12[11]);
     }
     else
-        pair_args(&p, &s, sanitize_pf(pf), 0, 0, 0, &pu, &su);
-    ft_general(&p, &s, &pu, &su, out6);
+        pair_args(&p, &s, sanitize_pf(pf), 0, zax, 0, &pu, &su);
+    if (zax)
+    {
+        /* Coil::computeForceTorque (src/Coil/ForceAndTorque/ComputeForceMethods.cxx:4-23) */
+        for (int i = 0; i < 6; ++i)
+            out6[i] = 0.0;
+        out6[2] = zaxis_value(&p, &s, &pu, &su, 1);
+    }
+    else
+        ft_general(&p, &s, &pu, &su, out6);
     return 0;
 }

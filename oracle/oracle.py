@@ -102,14 +102,14 @@ class Oracle:
         rc = self.lib.oracle_mutual_inductance(_ptr(_f64(prim)), _ptr(_f64(sec)), pf, _ptr(_i32(args), _ip),
                                                _ptr(out))
         if rc != 0:
-            raise ValueError("coaxial pair: the reference uses its z-axis formula")
+            raise ValueError("oracle pair evaluation failed (invalid coils or arguments)")
         return float(out[0])
 
     def force_torque(self, prim, sec, pf=5.0, args=None):
         out = np.zeros(6)
         rc = self.lib.oracle_force_torque(_ptr(_f64(prim)), _ptr(_f64(sec)), pf, _ptr(_i32(args), _ip), _ptr(out))
         if rc != 0:
-            raise ValueError("coaxial pair: the reference uses its z-axis formula")
+            raise ValueError("oracle pair evaluation failed (invalid coils or arguments)")
         return out
 
 

@@ -22,6 +22,10 @@ benchmark configurations' shapes:
   single_rect     the single RECTANGULAR coil configuration, 512 points, PF 5
   group_mixed     12 mixed-type coils, 96 points, PF 1, 3, 5, 7, 9
   pairs           24 RECTANGULAR/THIN arrangements of the pair configuration, PF 5
+  z_axis          coaxial arrangements of every coil-type combination (the reference's
+                  z-axis formulas, src/Coil/MInductance/CalculateMInductanceZAxis.cxx,
+                  src/Coil/ForceAndTorque/CalculateForceZAxis.cxx), a coaxial group, and
+                  self inductances (CalculateMInductanceZAxis.cxx:233-319)
   precision       precision arguments of 400 seeded coils at 6 PrecisionFactors, CPU and GPU
   pair_precision  pair arguments of 100 seeded pairs, CPU and pure-GPU
 """
@@ -127,6 +131,54 @@ def main():
     g["pairs_angles"] = np.stack([py, pz, sy, sz])
     g["pairs_M"] = R.m_arrangements(prim, sec, ppos, spos, py, pz, sy, sz, pf=5.0)
     g["pairs_FT"] = R.ft_arrangements(prim, sec, ppos, spos, py, pz, sy, sz, pf=5.0)
+
+    # --- coaxial pairs: the reference's z-axis formulas (every coil-type combination) ------------
+    # 6 arrangements per combination: 4 coaxial (both y angles 0, centres on the z axis, any z
+    # angles) and 2 off-axis ones that take the general formula; PF 3 and 5
+    ztypes = [(0.1, 0.05, 0.1, 200), (0.08, 0.0, 0.12, 150), (0.12, 0.04, 0.0, 120), (0.06, 0.0, 0.0, 80)]
+    zr = np.random.default_rng(51)
+    zp_, zs_, zpp, zsp, zang, zm3, zm5, zft = [], [], [], [], [], [], [], []
+    for pd in ztypes:
+        for sd in ztypes:
+            prim_row = coil_row(*pd[:3], pd[3], 2.0)
+            sec_row = coil_row(*sd[:3], sd[3], 3.0)
+            ppos = np.zeros((6, 3))
+            ppos[:, 2] = zr.uniform(-0.1, 0.1, 6)
+            dz = zr.choice([-1.0, 1.0], 6) * zr.uniform(0.15, 0.4, 6)
+            spos = ppos + np.stack([np.zeros(6), np.zeros(6), dz], axis=1)
+            spos[4:, 0] += zr.uniform(0.01, 0.05, 2)
+            py, sy = np.zeros(6), np.zeros(6)
+            sy[5] = 0.3
+            pz, sz = zr.uniform(0, 2 * np.pi, 6), zr.uniform(0, 2 * np.pi, 6)
+            zp_.append(prim_row)
+            zs_.append(sec_row)
+            zpp.append(ppos)
+            zsp.append(spos)
+            zang.append(np.stack([py, pz, sy, sz]))
+            zm3.append(R.m_arrangements(prim_row, sec_row, ppos, spos, py, pz, sy, sz, pf=3.0))
+            zm5.append(R.m_arrangements(prim_row, sec_row, ppos, spos, py, pz, sy, sz, pf=5.0))
+            zft.append(R.ft_arrangements(prim_row, sec_row, ppos, spos, py, pz, sy, sz, pf=5.0))
+    g["zax_prim"], g["zax_sec"], g["zax_prim_pos"], g["zax_sec_pos"] = map(np.array, (zp_, zs_, zpp, zsp))
+    g["zax_angles"], g["zax_M_pf3"], g["zax_M_pf5"], g["zax_FT_pf5"] = map(np.array, (zang, zm3, zm5, zft))
+
+    # coaxial group: 4 stacked coils of different types, a RECTANGULAR secondary moving along
+    # the axis (first 5 arrangements) and off it (last 3), PF 4
+    zg = np.array([coil_row(*ztypes[i][:3], ztypes[i][3], 1.5, 0.0, (0.0, 0.0, 0.3 * i - 0.45)) for i in range(4)])
+    zsec = coil_row(0.05, 0.02, 0.06, 90, 2.5)
+    zgs = np.zeros((8, 3))
+    zgs[:, 2] = [-0.75, -0.6, 0.6, 0.75, 0.9, -0.7, 0.65, 0.8]
+    zgs[5:, 1] = [0.02, 0.04, 0.01]
+    zgy = np.zeros(8)
+    zgz = np.linspace(0.0, 1.0, 8)
+    g["zgrp_coils"], g["zgrp_sec"], g["zgrp_sec_pos"], g["zgrp_angles"] = zg, zsec, zgs, np.stack([zgy, zgz])
+    g["zgrp_M"] = R.group_m_arrangements(zg, zsec, zgs, zgy, zgz, pf=4.0)
+    g["zgrp_FT"] = R.group_ft_arrangements(zg, zsec, zgs, zgy, zgz, pf=4.0)
+
+    # self inductance (Coil::computeAndSetSelfInductance) of RECTANGULAR, THIN and FLAT coils
+    sic = np.array([coil_row(0.1, 0.05, 0.1, 200), coil_row(0.03, 0.03, 0.12, 3600), coil_row(0.08, 0.0, 0.12, 150),
+                    coil_row(0.12, 0.04, 0.0, 120), coil_row(0.5, 0.1, 0.05, 10)])
+    g["self_coils"] = sic
+    g["self_L"] = np.array([[R.self_inductance(c, pf=pf) for pf in (3.0, 5.0)] for c in sic])
 
     # --- precision arguments ------------------------------------------------------------------
     rng = np.random.default_rng(41)

@@ -64,12 +64,14 @@ def test_parallel_axes_golden(ccoil, golden, oracle):
         pytest.skip("no parallel-axes fixture")
     done = 0
     for p, s, m in zip(golden["pa_prim"], golden["pa_sec"], golden["pa_M"]):
-        if oracle.z_axis_case(p, s):
-            continue  # the reference uses its z-axis formulas there
+        # coaxial rows take the z-axis formulas, as in the reference
         prim, sec = rows_to_coil(ccoil, p), rows_to_coil(ccoil, s)
+        # coaxial rows: the reference's -ffast-math build of its closed-form z-axis
+        # formula differs from strict evaluation up to ~5e-11 (tests/test_zaxis_gpu.py)
+        tol = 1e-10 if oracle.z_axis_case(p, s) else TOL
         for j, pf in enumerate((3.0, 5.0)):
             got = ccoil.Coil.compute_mutual_inductance(prim, sec, ccoil.PrecisionFactor(pf))
-            assert abs(got - m[j]) <= TOL * abs(m[j]), (p, s, pf, got, m[j])
+            assert abs(got - m[j]) <= tol * abs(m[j]), (p, s, pf, got, m[j])
         done += 1
     assert done > 10
 
