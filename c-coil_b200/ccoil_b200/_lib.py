@@ -94,6 +94,7 @@ def lib():
     L.ccoil_b_field_adjoint.argtypes = [dp, pp, ctypes.c_int, vp, ctypes.c_longlong, vp, vp, vp]
     L.ccoil_pair_arrangements.argtypes = [cp, ctypes.c_int, cp, pp, vp, vp, ctypes.c_longlong, ctypes.c_int,
                                           ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, vp]
+    L.ccoil_self_inductances.argtypes = [cp, pp, ctypes.c_int, vp, vp]
     L.ccoil_pair_arrangements_zaxis.argtypes = [cp, ctypes.c_int, cp, pp, pp, vp, vp, ctypes.c_longlong,
                                                 ctypes.c_int, ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong),
                                                 ctypes.c_int, vp]

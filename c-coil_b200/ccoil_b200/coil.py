@@ -425,6 +425,34 @@ class Coil:
                                   precision_factor or PrecisionFactor(), compute_method, _lib.PAIR_FORCE_TORQUE,
                                   precision_mode)
 
+    # --- self inductance ----------------------------------------------------------------------
+    def compute_and_set_self_inductance(self, precision_factor=None):
+        """Coil::computeAndSetSelfInductance (ComputeMInductanceMethods.cxx:55-81): the coil's self
+        inductance at its z-axis pair arguments with itself; stored and returned."""
+        self._self_inductance = float(Coil.compute_all_self_inductances([self], precision_factor)[0])
+        return self._self_inductance
+
+    def get_self_inductance(self):
+        return getattr(self, "_self_inductance", 0.0)
+
+    @staticmethod
+    def compute_all_self_inductances(coils, precision_factor=None):
+        """Self inductances of many coils in one launch (no counterpart in the reference)."""
+        pf = _factor(precision_factor or PrecisionFactor())
+        structs, args = [], []
+        for c in coils:
+            a = CoilPairArguments.get_appropriate_coil_pair_arguments(c, c, pf, ComputeMethod.CPU_ST,
+                                                                      z_axis_case=True)
+            structs.append(c.struct(a.primary_precision))
+            args += [a.primary_precision.to_struct(), a.secondary_precision.to_struct()]
+        out = np.zeros(len(structs))
+        if not structs:
+            return out
+        arr = (_lib.CoilStruct * len(structs))(*structs)
+        pa = (_lib.PrecisionArgsStruct * len(args))(*args)
+        check(lib().ccoil_self_inductances(arr, pa, len(structs), out.ctypes.data_as(ctypes.c_void_p), None))
+        return out
+
     def _pose_row(self):
         return self.get_position_vector(), self._s.y_axis_angle, self._s.z_axis_angle
 

@@ -245,6 +245,18 @@ int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int primary_cou
                                   const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
                                   double *out, long long *z_axis_count, int memory, void *stream);
 
+/* Self inductance of `count` coils (Coil::computeAndSetSelfInductance,
+ * src/Coil/MInductance/ComputeMInductanceMethods.cxx:55-81):
+ * pair_precisions[2c] and [2c+1] are the coil's pair arguments with itself in
+ * the z-axis case (ccoil_pair_arguments(&coil, &coil, pf, 0, 1, 0, ...)).
+ * RECTANGULAR and THIN coils use the closed form of Coil::calculateSelfInductance
+ * (src/Coil/MInductance/CalculateMInductanceZAxis.cxx:233-319), FLAT coils the
+ * coaxial mutual inductance of the centred coil with itself; a FILAMENT is
+ * rejected (CCOIL_ERR_INVALID_ARGUMENT: the integral diverges).  out: host
+ * array of count doubles; synchronous on `stream`. */
+int ccoil_self_inductances(const ccoil_coil_t *coils, const ccoil_precision_args_t *pair_precisions, int count,
+                           double *out, void *stream);
+
 /* ------------------------------------------------------------------------ *
  * Batched independent systems                                               *
  * ------------------------------------------------------------------------ */

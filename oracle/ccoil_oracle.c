@@ -1040,3 +1040,73 @@ int oracle_force_torque(const double *pc, const double *sc, double pf, const int
         ft_general(&p, &s, &pu, &su, out6);
     return 0;
 }
+
+/* Self inductance, Coil::computeAndSetSelfInductance
+ * (src/Coil/MInductance/ComputeMInductanceMethods.cxx:55-81): the centred coil,
+ * its z-axis pair arguments with itself (or args12); FLAT through the coaxial
+ * mutual inductance with itself, RECTANGULAR / THIN through the closed form of
+ * Coil::calculateSelfInductance (src/Coil/MInductance/CalculateMInductanceZAxis.cxx:233-319).
+ * Returns 1 for a FILAMENT (divergent integral). */
+int oracle_self_inductance(const double *c, double pf, const int *args12, double *out)
+{
+    build_tables();
+    double row[11];
+    for (int i = 0; i < 11; ++i)
+        row[i] = c[i];
+    row[6] = row[7] = row[8] = row[9] = row[10] = 0.0;
+    OCoil k;
+    make_coil(row, &k);
+    if (k.type == FILAMENT)
+        return 1;
+    OArgs pu, su;
+    if (args12)
+    {
+        pu = make_args(args12[0], args12[1], args12[2], args12[3], args12[4], args12[5]);
+        su = make_args(args12[6], args12[7], args12[8], args12[9], args12[10], args12[11]);
+    }
+    else
+        pair_args(&k, &k, sanitize_pf(pf), 0, 1, 0, &pu, &su);
+    if (k.type == FLAT)
+    {
+        *out = zaxis_value(&k, &k, &pu, &su, 0);
+        return 0;
+    }
+    double tb = k.a / pu.tB, ab = PI / pu.aB, rb = 1.0 / su.tB;
+    double constant = MI_REDUCED * k.J * tb * ab * rb * 2 * 0.125;
+    double b2 = k.b * k.b;
+    double *cs = angular_cos(&pu);
+    double sum = 0.0;
+    for (int bR = 0; bR < su.tB; ++bR)
+    {
+        double blockR = k.R + rb * k.a * (bR + 0.5);
+        for (int iR = 0; iR < su.tI; ++iR)
+        {
+            double r = blockR + (rb * k.a * 0.5) * g_pos[su.tI - 1][iR];
+            double wR = g_wts[su.tI - 1][iR];
+            for (int bT = 0; bT < pu.tB; ++bT)
+            {
+                double blockT = k.R + tb * (bT + 0.5);
+                for (int iT = 0; iT < pu.tI; ++iT)
+                {
+                    double t = blockT + (tb * 0.5) * g_pos[pu.tI - 1][iT];
+                    double wT = g_wts[pu.tI - 1][iT];
+                    double c0 = constant * wR * wT;
+                    double A = 2 * t * r, B = t * t + r * r;
+                    for (int bP = 0; bP < pu.aB; ++bP)
+                        for (int iP = 0; iP < pu.aI; ++iP)
+                        {
+                            double wP = g_wts[pu.aI - 1][iP];
+                            double cc = cs[bP * pu.aI + iP];
+                            double C = B - A * cc;
+                            double D = sqrt(C), E = sqrt(C + b2);
+                            double F = k.b / D, G = sqrt(F * F + 1.0), H = log(F + G);
+                            sum += c0 * wP * A * cc * (D - E + k.b * H);
+                        }
+                }
+            }
+        }
+    }
+    free(cs);
+    *out = sum * 2 * PI * k.N / (k.I * k.b);
+    return 0;
+}

@@ -56,6 +56,7 @@ class Oracle:
         L.oracle_mutual_inductance.argtypes = [_dp, _dp, _d, _ip, _dp]
         L.oracle_force_torque.argtypes = [_dp, _dp, _d, _ip, _dp]
         L.oracle_z_axis_case.argtypes = [_dp, _dp]
+        L.oracle_self_inductance.argtypes = [_dp, _d, _ip, _dp]
 
     def legendre(self, order):
         p, w = np.zeros(order), np.zeros(order)
@@ -103,6 +104,13 @@ class Oracle:
                                                _ptr(out))
         if rc != 0:
             raise ValueError("oracle pair evaluation failed (invalid coils or arguments)")
+        return float(out[0])
+
+    def self_inductance(self, coil, pf=5.0, args=None):
+        out = np.zeros(1)
+        rc = self.lib.oracle_self_inductance(_ptr(_f64(coil)), pf, _ptr(_i32(args), _ip), _ptr(out))
+        if rc != 0:
+            raise ValueError("a filament has no self inductance (divergent integral)")
         return float(out[0])
 
     def force_torque(self, prim, sec, pf=5.0, args=None):

@@ -151,3 +151,13 @@ def test_oracle_z_axis_formulas_against_reference(golden, oracle):
                 worst_slow = max(worst_slow, e)
     assert worst_fast < 1e-10, worst_fast
     assert worst_slow < 1e-12, worst_slow
+
+
+def test_oracle_self_inductance_against_reference(golden, oracle):
+    """Coil::computeAndSetSelfInductance restated (RECTANGULAR, THIN closed form; FLAT
+    through the coaxial mutual inductance with itself) against the compiled reference."""
+    for c, L in zip(golden["self_coils"], golden["self_L"]):
+        for j, pf in enumerate((3.0, 5.0)):
+            assert abs(oracle.self_inductance(c, pf=pf) - L[j]) <= 1e-12 * abs(L[j]), (c, pf)
+    with pytest.raises(ValueError):
+        oracle.self_inductance(np.array([0.1, 0.0, 0.0, 10, 1.0, 0, 0, 0, 0, 0, 0]))
