@@ -288,16 +288,11 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    from ccoil_b200 import distributed as D
+    barrier = D.barrier
 
     def max_over_ranks(x):
-        if world == 1:
-            return float(x)
-        t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return D.max_over_ranks(x, dev)
 
     rows, _ = workloads.group_config(coils=a.coils, points=1)
     coils = workloads.coils_from_rows(rows, a.pf)
