@@ -7,6 +7,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 namespace ccoil
@@ -26,7 +27,11 @@ struct DeviceBuffer
     void release()
     {
         if (ptr)
-            cudaFree(ptr);
+        {
+            cudaDeviceSynchronize();
+            cudaFreeAsync(ptr, nullptr);
+            cudaStreamSynchronize(nullptr);
+        }
         ptr = nullptr;
         bytes = 0;
     }
@@ -54,16 +59,62 @@ int cudaFail(cudaError_t e, const char *what)
 
 namespace
 {
+std::mutex g_poolMutex;
+constexpr int kMaxDevices = 64;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+} // namespace
+
+cudaError_t scratchAlloc(void **p, size_t bytes, cudaStream_t st)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    if (dev < 0 || dev >= kMaxDevices)
+        return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_poolMutex);
+        if (!g_pools[dev])
+        {
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&g_pools[dev], &props);
+            if (e != cudaSuccess)
+            {
+                g_pools[dev] = nullptr;
+                return e;
+            }
+            unsigned long long keep = 1ULL << 32;
+            e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (e != cudaSuccess)
+                return e;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+namespace
+{
+// plan buffers: allocated and released in the order of the legacy default
+// stream, which waits for all blocking streams; release waits for the device
+// so that no kernel on any stream still reads the buffer
 int DeviceBuffer::reserve(size_t n)
 {
     if (n <= bytes)
         return CCOIL_OK;
     release();
-    cudaError_t e = cudaMalloc(&ptr, n);
+    cudaError_t e = scratchAlloc(&ptr, n, nullptr);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(nullptr);
     if (e != cudaSuccess)
     {
         ptr = nullptr;
-        return cudaFail(e, "cudaMalloc");
+        return cudaFail(e, "device buffer");
     }
     bytes = n;
     return CCOIL_OK;

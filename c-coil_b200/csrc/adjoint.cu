@@ -30,6 +30,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -89,7 +91,8 @@ __global__ void __launch_bounds__(kAdjThreads) adjointKernel(const unsigned char
             P[i] = points[3 * p + i];
             v[i] = gradB[3 * p + i];
         }
-    for (int c = 0; c < ncoils; ++c)
+    // blockIdx.x: a tile of kAdjPoints points; blockIdx.y (grid-strided): the coil
+    for (int c = blockIdx.y; c < ncoils; c += gridDim.y)
     {
         const unsigned char *base = blob + offsets[c];
         const AdjCoil &C = *reinterpret_cast<const AdjCoil *>(base);
@@ -247,13 +250,19 @@ void putBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
     blob.insert(blob.end(), c, c + n);
 }
 
-struct DBuf
+struct DBuf  // stream-ordered temporary from the library's memory pool
 {
     void *p = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t alloc(size_t bytes, cudaStream_t s)
+    {
+        st = s;
+        return scratchAlloc(&p, bytes, s);
+    }
     ~DBuf()
     {
         if (p)
-            cudaFree(p);
+            cudaFreeAsync(p, st);
     }
 };
 } // namespace
@@ -336,11 +345,11 @@ extern "C" int ccoil_b_field_adjoint(const double *params, const ccoil_precision
     if (blocks > (1LL << 24))
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "point_count too large for the adjoint's partial sums");
     DBuf dBlob, dOff, dPartial;
-    cudaError_t e = cudaMalloc(&dBlob.p, blob.size());
+    cudaError_t e = dBlob.alloc(blob.size(), st);
     if (e == cudaSuccess)
-        e = cudaMalloc(&dOff.p, sizeof(long long) * offsets.size());
+        e = dOff.alloc(sizeof(long long) * offsets.size(), st);
     if (e == cudaSuccess)
-        e = cudaMalloc(&dPartial.p, sizeof(double) * 9 * coil_count * blocks);
+        e = dPartial.alloc(sizeof(double) * 9 * coil_count * blocks, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dBlob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
@@ -350,10 +359,9 @@ extern "C" int ccoil_b_field_adjoint(const double *params, const ccoil_precision
     if (point_count == 0)
         e = cudaMemsetAsync(dPartial.p, 0, sizeof(double) * 9 * coil_count, st);
     else
-        adjointKernel<<<(unsigned)blocks, kAdjThreads, 0, st>>>(static_cast<const unsigned char *>(dBlob.p),
-                                                                 static_cast<const long long *>(dOff.p), coil_count,
-                                                                 points, grad_b, point_count,
-                                                                 static_cast<double *>(dPartial.p));
+        adjointKernel<<<dim3((unsigned)blocks, (unsigned)std::min(coil_count, 65535)), kAdjThreads, 0, st>>>(
+            static_cast<const unsigned char *>(dBlob.p), static_cast<const long long *>(dOff.p), coil_count, points,
+            grad_b, point_count, static_cast<double *>(dPartial.p));
     if (e == cudaSuccess)
         e = cudaGetLastError();
     if (e == cudaSuccess)
@@ -362,6 +370,6 @@ extern "C" int ccoil_b_field_adjoint(const double *params, const ccoil_precision
     if (e == cudaSuccess)
         e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cudaStreamSynchronize(st);  // the temporaries are freed on return
+        e = cudaStreamSynchronize(st);  // results in grad_params when the call returns
     return e == cudaSuccess ? CCOIL_OK : cudaFail(e, "adjoint");
 }

@@ -97,6 +97,13 @@ void setError(const std::string &msg);
 int fail(int status, const std::string &msg);
 int failMessage(int status, const char *msg);  // same, without building a std::string
 
+// Device memory for the library's temporaries and plans, from a memory pool of
+// the library's own (one per device, created on first use) that keeps up to
+// 4 GiB of freed blocks for reuse: after the first calls, allocating and
+// freeing costs no driver mapping work and no device-wide synchronisation.
+// scratchAlloc/cudaFreeAsync are ordered on `st`.
+cudaError_t scratchAlloc(void **p, size_t bytes, cudaStream_t st);
+
 // kernels (fields.cu)
 struct FieldLaunch
 {

@@ -827,8 +827,8 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
 
 #include "zaxis.cuh"
 
-// Stream-ordered temporary (cudaMallocAsync / cudaFreeAsync from the device's
-// default pool): no device-wide synchronisation per call
+// Stream-ordered temporary from the library's memory pool: no device-wide
+// synchronisation and no driver mapping work per call
 struct DevBuf
 {
     void *p = nullptr;
@@ -836,7 +836,7 @@ struct DevBuf
     cudaError_t alloc(size_t bytes, cudaStream_t s)
     {
         st = s;
-        return cudaMallocAsync(&p, bytes, s);
+        return scratchAlloc(&p, bytes, s);
     }
     ~DevBuf()
     {
@@ -946,7 +946,7 @@ extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int 
             e = dOut.alloc(sizeof(double) * width * count, st);
     }
     if (e != cudaSuccess)
-        return cudaFail(e, "cudaMallocAsync");
+        return cudaFail(e, "scratch allocation");
     e = cudaMemcpyAsync(dBlob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dOff.p, offsets.data(), sizeof(long long) * offsets.size(), cudaMemcpyHostToDevice, st);

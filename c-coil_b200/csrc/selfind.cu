@@ -133,7 +133,7 @@ void buildSelf(const Coil &k, const PrecisionArgs &p, const PrecisionArgs &s, st
     put(blob, f.data(), sizeof(double) * f.size());
 }
 
-// stream-ordered temporary (cudaMallocAsync / cudaFreeAsync)
+// stream-ordered temporary from the library's memory pool
 struct Buf
 {
     void *p = nullptr;
@@ -141,7 +141,7 @@ struct Buf
     cudaError_t alloc(size_t bytes, cudaStream_t s)
     {
         st = s;
-        return cudaMallocAsync(&p, bytes, s);
+        return scratchAlloc(&p, bytes, s);
     }
     ~Buf()
     {
