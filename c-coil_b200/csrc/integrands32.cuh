@@ -88,7 +88,7 @@ __device__ __forceinline__ float rsqrtNR(float x)
 
 // asinh(u): the Maclaurin series sum_n (-1)^n (2n)! / (4^n (n!)^2 (2n+1)) u^(2n+1)
 // through n = 6 when every lane of the warp has |u| < 0.25 (truncation below
-// 6e-11 relative there), CUDA's asinhf otherwise
+// 6e-11 relative there); asinhLarge beyond (CUDA's asinhf past 1e18)
 __device__ __forceinline__ float asinhSmall(float u)
 {
     const float u2 = u * u;
@@ -101,12 +101,50 @@ __device__ __forceinline__ float asinhSmall(float u)
     return fmaf(p * u2, u, u);
 }
 
+// asinh(u) for 0.25 <= |u| < 1e18: log(x) with x = |u| + sqrt(1 + u^2) carried
+// as x_hi + x_lo (one Newton step on the square root, the exact residual of
+// 1 + u^2 and of the sum), then log(x_hi) by exponent reduction to
+// m in [sqrt(1/2), sqrt(2)) and log(m) = 2 atanh(f), f = (m - 1) / (m + 1), as
+// 2 (f + f^3/3 + ... + f^9/9) (|f| <= 0.1716: truncation below 3e-9 relative),
+// plus x_lo / x_hi; ln 2 is split into a high part exact in e ln2_hi and a low
+// part (Cody and Waite).  About 1-2 ulp over the range.
+__device__ __forceinline__ float asinhLarge(float u)
+{
+    const float a = fabsf(u);
+    const float y = fmaf(a, a, 1.0f);
+    const float ylo = fmaf(a, a, 1.0f - y);  // 1 + a^2 - y (exact while y < 2; negligible beyond)
+    const float rs = rsqrtNR(y);
+    float sq = y * rs;
+    sq = fmaf(0.5f * fmaf(-sq, sq, y), rs, sq);
+    const float ds = (fmaf(-sq, sq, y) + ylo) * (0.5f * rs);
+    const float xh = sq + a;  // sq >= a: exact rounding error below
+    const float xl = (a - (xh - sq)) + ds;
+    const int i = __float_as_int(xh);
+    const int e = (i - 0x3f3504f3) >> 23;
+    const float m = __int_as_float(i - (e << 23));
+    const float g = m - 1.0f;  // exact
+    const float t = 2.0f + g;
+    const float tl = g - (t - 2.0f);  // exact rounding error of t
+    const float rc = rcpApprox(t);
+    const float q = g * rc;
+    const float f = fmaf(rc, fmaf(-q, t, g) - q * tl, q);
+    const float z = f * f;
+    const float p = fmaf(fmaf(fmaf(0.11111111f, z, 0.14285715f), z, 0.2f), z, 0.33333334f);
+    const float f2 = 2.0f * f;
+    const float logm = fmaf(f2 * z, p, f2);
+    const float ef = (float)e;
+    const float r = fmaf(ef, 0.693145751953125f, fmaf(ef, 1.42860682e-06f, logm + xl * rcpApprox(xh)));
+    return copysignf(r, u);
+}
+
 __device__ __forceinline__ float asinhFast(float u)
 {
     const bool small = fabsf(u) < 0.25f;
     if (__all_sync(__activemask(), small))
         return asinhSmall(u);
-    return small ? asinhSmall(u) : asinhf(u);
+    if (small)
+        return asinhSmall(u);
+    return fabsf(u) < 1e18f ? asinhLarge(u) : asinhf(u);
 }
 
 __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame &f)
