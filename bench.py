@@ -10,6 +10,7 @@ PrecisionArguments.  Seeded synthetic data; no dataset is involved.
     python bench.py --impl reference        # the reference's own CPU_MT code on this host
     python bench.py --workload batched      # 2,048 independent systems, one persistent launch per step
     python bench.py --workload adjoint      # forward + backward of a B-field loss (64 coils)
+    python bench.py --workload pf-sweep     # the group at PrecisionFactor 1, 3, 5, 7, 9
 
 Under torchrun every rank evaluates its own 2^20 points (weak scaling, no
 collective on the data path); times are device times (CUDA events), max over
@@ -48,9 +49,10 @@ def parse():
                     help="coil-pair arrangements per GPU for the M and F/T part (0 skips it)")
     ap.add_argument("--cpu-sample-arrangements", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="group", choices=["group", "batched", "adjoint"],
+    ap.add_argument("--workload", default="group", choices=["group", "batched", "adjoint", "pf-sweep"],
                     help="group: the headline coil-group fields + pair arrangements; batched: many independent "
-                         "systems in one persistent launch; adjoint: forward + backward of the B-field loss")
+                         "systems in one persistent launch; adjoint: forward + backward of the B-field loss; "
+                         "pf-sweep: the group at PrecisionFactor 1, 3, 5, 7, 9 (2^18 points)")
     ap.add_argument("--systems", type=int, default=2048, help="independent systems of the batched workload")
     return ap.parse_args()
 
@@ -379,6 +381,64 @@ def bench_adjoint(a):
     print(json.dumps(line))
 
 
+def bench_pf_sweep(a):
+    """The coil group at PrecisionFactor 1, 3, 5, 7 and 9: throughput of A, B and G in FP64 and
+    FP32-compensated, and the FP32c error against FP64, at 2^18 points."""
+    import torch
+    import ccoil_b200 as cc
+    from ccoil_b200 import opcount, workloads
+    dev = torch.device("cuda", 0)
+    npts = 1 << 18
+    rows, _ = workloads.group_config(coils=a.coils, points=1)
+    pts_host = workloads.points_cube(npts, seed=1002)
+    pts = torch.from_numpy(pts_host).to(dev)
+    near, band = (torch.from_numpy(m).to(dev) for m in winding_masks(rows, pts_host))
+    flush = flush_l2(torch, dev)
+    sweep = []
+    for pf in (1.0, 3.0, 5.0, 7.0, 9.0):
+        coils = workloads.coils_from_rows(rows, pf)
+        group = cc.CoilGroup(coils, cc.PrecisionFactor(pf))
+        entry = {"precision_factor": pf, "nodes_per_point": opcount.group_nodes_per_point(coils)}
+        outs = {}
+        for mode in (cc.PrecisionMode.FP64, cc.PrecisionMode.FP32_COMPENSATED):
+            key = "fp64" if int(mode) == 0 else "fp32c"
+            step_ms = 0.0
+            for name, f in FIELDS:
+                plan = group.plan(f, mode)
+                out = plan(pts)
+                for _ in range(max(a.warmup, 3) - 1):
+                    plan(pts, out=out)
+                torch.cuda.synchronize()
+                ms = 0.0
+                for _ in range(a.steps):
+                    flush()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    plan(pts, out=out)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    ms += e0.elapsed_time(e1)
+                step_ms += ms / a.steps
+                outs[(key, name)] = out.clone()
+                plan.close()
+            entry[key] = {"ms_per_step": step_ms, "value": len(FIELDS) * a.coils * npts / (step_ms * 1e-3)}
+        entry["fp32c_speedup_vs_fp64"] = entry["fp64"]["ms_per_step"] / entry["fp32c"]["ms_per_step"]
+        entry["fp32c_rel_err_vs_fp64_away"] = {
+            name: rel_err_stats(outs[("fp32c", name)], outs[("fp64", name)], ~band if f == 3 else ~near)
+            for name, f in FIELDS}
+        sweep.append(entry)
+    head = [e for e in sweep if e["precision_factor"] == 5.0][0]
+    line = {"metric": "coil-point field evals/s over the PrecisionFactor sweep (A+B+G, FP32c)",
+            "value": head["fp32c"]["value"], "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": head["fp32c"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (compensated) + f64", "data": "synthetic (seeded)",
+            "config": {"workload": "coil group: 128 mixed coils, 262144 points in a 2 m cube, A+B+G, "
+                                   "PrecisionFactor 1, 3, 5, 7, 9 (value: PF 5)", "coils": a.coils,
+                       "points": npts, "l2": "flushed between timed launches (256 MiB write)"},
+            "sweep": sweep, "gpu_launches": 2 * len(FIELDS) * a.steps * 5}
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -389,6 +449,9 @@ def main():
         return
     if a.workload == "adjoint":
         bench_adjoint(a)
+        return
+    if a.workload == "pf-sweep":
+        bench_pf_sweep(a)
         return
 
     import torch

@@ -14,8 +14,12 @@
 //   asinh(top/rho) - asinh(bot/rho) (vector potential)
 //                  -> asinh(dD / (top s2 + bot s1)) outside the slab,
 //                     asinh((top s2 - bot s1) / rho^2) inside it
-//   RZ gradient node -> p cos (top G1^3 - bot G2^3) (equal node by node to the
-//                     reference's 1/M^2 form, without its cancellation)
+//   RZ gradient node (fast) -> p [c (T1 + Y) - k (2 Y + T1)], where
+//                     T1 = top G1^3 - bot G2^3, Y = (top G1 - bot G2) / rho^2 and
+//                     k = p r sin^2 / rho^2 (in [0, 1]): equal node by node to the
+//                     reference's (p / M^2)(top L1 (O J1 + N) - bot L2 (O J2 + N)),
+//                     via N = c rho^4 - p r s^2 rho^2 and O = c rho^2 - 2 p r s^2,
+//                     without its 1/rho^4 cancellation
 // and the azimuthal tables hold w*cos exactly antisymmetric about pi/2 in FP32.
 
 
@@ -301,11 +305,20 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 const float dg = dDf * gg * gg * rcpApprox(s);       // G2 - G1
                 const float dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));  // G1^3 - G2^3
                 const float g13 = g1 * g1 * g1;
-                const float rzv = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
+                // T1 = top G1^3 - bot G2^3 and Y = (top G1 - bot G2) / rho^2, each in
+                // its cancellation-free form for a point outside / inside the slab
+                const float T1 = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
+                const float rho2 = fmaf(b2, nd.omc, qf);
+                const float t1 = topf * g1, t2 = botf * g2;
+                const float yn = same ? dDf * gg * gg : (t1 - t2);
+                const float yd = same ? (t1 + t2) : rho2;
+                const float Y = yn * rcpApprox(yd);
+                // k = p r sin^2 / rho^2 = (b2 / 2)(1 - c)(1 + c) / rho^2
+                const float ks = (0.5f * b2) * (nd.omc * (2.0f - nd.omc)) * rcpApprox(rho2);
                 acc.a.add(nd.wc * dg);
                 acc.b.add(nd.wc * fmaf(pf, nd.omc, rmp) * dg3);   // (r - p cos)
                 acc.d.add(nd.w * fmaf(rf, nd.omc, pmr) * dg3);    // (p - r cos)
-                acc.c.add(nd.wc * rzv);
+                acc.c.add(fmaf(nd.wc, T1 + Y, -nd.w * ks * fmaf(2.0f, Y, T1)));
             });
             const double w = t.y * t.x;
             rphi += w / r * (a0.a.value() + a1.a.value());

@@ -108,3 +108,17 @@ def test_repeatable(ccoil):
     b = evaluate(ccoil, coils, pts, 1, ccoil.PrecisionMode.FP32_COMPENSATED)
     # the near-field pass adds with FP64 atomics: run-to-run differences stay at rounding level
     assert rel_err(a, b).max() < 1e-14
+
+
+@pytest.mark.parametrize("pf", [1.0, 3.0, 7.0])
+def test_gradient_across_precision_factors(ccoil, pf):
+    """The FP32 gradient integrands equal the reference's node by node, so the two
+    paths agree at every PrecisionFactor, including the coarse ones where a
+    different but equivalent integrand would differ by its quadrature error."""
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(16, seed=91)
+    pts = workloads.points_cube(8192, seed=92)
+    coils = workloads.coils_from_rows(rows, pf)
+    f64, f32 = (evaluate(ccoil, coils, pts, 3, m) for m in modes(ccoil))
+    e = rel_err(f32, f64)[~gradient_band(rows, pts)]
+    assert np.median(e) < 1e-7 and e.max() < 1e-5, (pf, np.median(e), e.max())
