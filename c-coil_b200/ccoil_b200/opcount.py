@@ -34,7 +34,7 @@ OPS_PER_NODE_64 = {
 OPS_PER_NODE_32 = {
     (0, True): (26, 3), (0, False): (6, 1),
     (1, True): (28, 3), (1, False): (15, 1),
-    (3, True): (44, 3), (3, False): (33, 1),
+    (3, True): (60, 5), (3, False): (33, 1),
 }
 # algorithmic flops per node: every operation of the reference integrand counts one
 FLOPS_PER_NODE = {k: sum(v) for k, v in OPS_PER_NODE_64.items()}
