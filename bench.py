@@ -629,6 +629,19 @@ def main():
             line["arrangements"]["fp32c_speedup_vs_fp64"] = {
                 q: arr["fp64"][q]["ms"] / arr["fp32c"][q]["ms"] for q in ("M", "FT")}
             line["arrangements"]["fp32c_rel_err_vs_fp64"] = arr["errors"]
+        if rates is not None and "fp64" in arr:
+            # FP64 pipe model of the arrangement kernels: every (secondary node, primary
+            # node) pair evaluates the reference's A (M) or B (F/T) fast node
+            pairs_per_arr = arr["secondary_nodes"] * arr["primary_nodes"]
+            roof = {}
+            for q, fidx in (("M", 0), ("FT", 1)):
+                am, dv, sq, lg = opcount.OPS_PER_NODE_64[(fidx, True)]
+                slots = pairs_per_arr * (am + dv * rates[0] / rates[1] + sq * rates[0] / rates[2] +
+                                         lg * rates[0] / rates[3]) * a.arrangements
+                t = arr["fp64"][q]["ms"] * 1e-3
+                roof[q] = {"achieved": 2.0 * slots / t / 1e12, "peak": 2.0 * rates[0] / 1e12, "unit": "TFLOP/s",
+                           "frac": slots / t / rates[0]}
+            line["arrangements"]["fp64_roofline"] = roof
         line["gpu_launches"] += 2 * a.steps * len(modes)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, cores, dt, desc = cpu_reference_rate(a, a.cpu_sample_points)
