@@ -346,10 +346,11 @@ __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *t
 // quadrature reads its tables from shared memory instead of through L1.
 //
 // FP32 (mutual inductance and force/torque only): the primary quadrature at a
-// secondary node runs in the FP32-compensated integrands, except for the warp
-// iterations in which some lane's node lies in the primary's near-field box,
-// which take the FP64 integrands (warp-uniform, so lanes do not diverge); the
-// secondary-node sums and the cross-lane reduction stay FP64.
+// secondary node runs in the FP32-compensated integrands, except for nodes in
+// the primary's near-field box: the warp defers those to a list in shared
+// memory and evaluates them with the FP64 integrands 32 at a time, so the FP64
+// work runs on full warps instead of dragging whole mixed iterations along;
+// the secondary-node sums and the cross-lane reduction stay FP64.
 template <int QTY, bool FP32>
 __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
@@ -360,6 +361,7 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
 {
     extern __shared__ __align__(16) unsigned char stagedPair[];
     __shared__ WarpPose warpPoses[4];
+    __shared__ int nearLists[4][64];  // FP32: each warp's deferred near-field secondary nodes
     if (stagedBytes > 0)
     {
         const int4 *src = reinterpret_cast<const int4 *>(blob + primOffsets[0]);
@@ -468,10 +470,12 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                 part[i] = 0.0;
             // every lane runs the same number of iterations (warp-uniform choices
             // below); a lane past the end evaluates the last node and drops it
-            for (int n0 = 0; n0 < nsec; n0 += 32)
-            {
-                const bool valid = n0 + lane < nsec;
-                const int n = valid ? n0 + lane : nsec - 1;
+            // One secondary node per lane.  mode 0: the FP64 kernel; mode 1: the FP32
+            // pass, which defers near-field nodes to the warp's list; mode 2: a batch
+            // of deferred nodes, in FP64, one per lane
+            int nNear = 0;
+            int *list = nearLists[threadIdx.x / 32];
+            auto node = [&](int n, bool valid, int mode) {
                 const int k = n % ph.s_na, lt_i = n / ph.s_na;
                 const int t = lt_i % ph.s_nt, l = lt_i / ph.s_nt;
                 const double2 L = sl[l], R = st[t];
@@ -487,7 +491,19 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                                      S.sp[1] + L.x * sA * sB + R.x * ringP[1], S.sp[2] + L.x * cA + R.x * ringP[2]};
                 const double w = 0.125 * R.x * L.y * R.y * A.w;
                 const Frame f = toCoilFrameAt(S.pos, S.Ti, q[0], q[1], q[2]);
-                const bool far = !FP32 || !__any_sync(0xffffffffu, valid && nearWinding(h, f));
+                const bool far = mode == 1;
+                if (mode == 1)
+                {
+                    const bool near = valid && nearWinding(h, f);
+                    const unsigned bal = __ballot_sync(0xffffffffu, near);
+                    if (bal)
+                    {
+                        if (near)
+                            list[nNear + __popc(bal & ((1u << lane) - 1u))] = n;
+                        nNear += __popc(bal);
+                        valid = valid && !near;
+                    }
+                }
                 if (QTY == 0)
                 {
                     double av;
@@ -632,7 +648,33 @@ __global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
                             part[3 + i] += dT[i];
                         }
                 }
-            }
+            };
+            if (!FP32)
+                for (int n0 = 0; n0 < nsec; n0 += 32)
+                    node(n0 + lane < nsec ? n0 + lane : nsec - 1, n0 + lane < nsec, 0);
+            else
+                for (int n0 = 0; n0 < nsec || nNear > 0;)
+                {
+                    if (nNear >= 32 || n0 >= nsec)
+                    {
+                        // 32 deferred near-field nodes (or the last few) in FP64
+                        __syncwarp();
+                        const bool v = lane < nNear;
+                        node(list[v ? lane : 0], v, 2);
+                        const int rest = nNear > 32 ? nNear - 32 : 0;
+                        const int moved = lane < rest ? list[32 + lane] : 0;
+                        __syncwarp();
+                        if (lane < rest)
+                            list[lane] = moved;
+                        __syncwarp();
+                        nNear = rest;
+                    }
+                    else
+                    {
+                        node(n0 + lane < nsec ? n0 + lane : nsec - 1, n0 + lane < nsec, 1);
+                        n0 += 32;
+                    }
+                }
 #pragma unroll
             for (int off = 16; off > 0; off /= 2)
 #pragma unroll
