@@ -16,9 +16,10 @@ square root or logarithm takes rate(FMA) / rate(op) slots, with the rates
 measured on the device by ccoil_measure_op_rates.
 
 FP32-compensated kernel.  Per node, the FP32 instructions (FMA pipe and ALU,
-including the four of each Kahan update) and the MUFU operations (reciprocal
-square root, reciprocal) of the kernel's own integrands, counted from
-integrands32.cuh; the kernel is bound by instruction issue (one FP32
+including the four of each Kahan update of the vector potential and field
+sums) and the MUFU operations (reciprocal square root, reciprocal) of the
+kernel's own integrands, counted from integrands32.cuh; the kernel is bound
+by instruction issue (one FP32
 instruction per lane and cycle, the FP32 FMA peak) or by MUFU, whichever is
 slower for the mix.
 """
@@ -30,11 +31,13 @@ OPS_PER_NODE_64 = {
     (1, True): (17, 3, 2, 0), (1, False): (11, 1, 1, 0),
     (3, True): (53, 6, 2, 0), (3, False): (33, 2, 1, 0),
 }
-# (field, fast) -> (FP32 FMA-pipe + ALU instructions, MUFU operations) per node
+# (field, fast) -> (FP32 FMA-pipe + ALU instructions, MUFU operations) per node:
+# the kernel evaluates mirror pairs of nodes, so these are half the count of
+# one pair step (both nodes' integrands and the pair's accumulation)
 OPS_PER_NODE_32 = {
-    (0, True): (26, 3), (0, False): (6, 1),
-    (1, True): (28, 3), (1, False): (15, 1),
-    (3, True): (60, 5), (3, False): (33, 1),
+    (0, True): (27, 3), (0, False): (4, 1),
+    (1, True): (26, 3), (1, False): (10.5, 1),
+    (3, True): (39.5, 5), (3, False): (16.5, 1),
 }
 # algorithmic flops per node: every operation of the reference integrand counts one
 FLOPS_PER_NODE = {k: sum(v) for k, v in OPS_PER_NODE_64.items()}

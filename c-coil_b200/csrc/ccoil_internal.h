@@ -57,14 +57,29 @@ struct SegmentDesc
     int coil;          // source coil index
 };
 
-// FP32 per-node tables appended after the FP64 tables (16 bytes per entry)
+// FP32 angular tables, appended after the FP64 tables (16 bytes per entry).
+// One entry describes a mirror pair of nodes: node k of the first half of
+// [0, pi] and node n-1-k (phi -> pi - phi), whose cosine is the exact negation.
+// The FP32 integrands evaluate both nodes and accumulate w c (f(c) - f(-c)) and
+// w (g(c) + g(-c)): far from the coil the two values agree to many digits and
+// their difference is exact in FP32, so the accumulation carries only the
+// antisymmetric part and needs no compensation.  Both nodes are formed from
+// the same per-thickness-node constants (Q + b2 omc and Q + b2 omcm), so the
+// rounding of those constants is common to the pair and cancels in the
+// difference.  With an odd node count the middle node (c = 0) is an entry of
+// its own with half its weight (evaluated twice).
 struct alignas(16) PhiNode32
 {
-    float wc;    // w_phi * cos(phi), exactly antisymmetric over the mirror node
-    float omc;   // 1 - cos(phi) = 2 sin^2(phi/2)
-    float c;     // cos(phi)
-    float w;     // w_phi
+    float wc;    // w_phi * c, c = (cos(phi_k) - cos(phi_{n-1-k})) / 2 (0 for the middle node)
+    float omc;   // 1 - cos(phi_k) = 2 sin^2(phi_k / 2)
+    float omcm;  // 1 - cos(phi_{n-1-k}) = 2 sin^2(phi_{n-1-k} / 2) (about 2 - omc)
+    float w;     // w_phi (halved for the middle node)
 };
+
+// Node order of the FP64 angular table in FP32 mode: position j holds node
+// j/2 (j even) or its mirror n-1-j/2 (j odd), so that any even-length slice of
+// the table covers whole mirror pairs; with odd n the middle node comes last.
+inline int pairOrderNode(int j, int n) { return (j & 1) ? n - 1 - (j >> 1) : (j >> 1); }
 
 // Host-built device tables for a coil set.
 struct SegmentSet
@@ -77,8 +92,11 @@ struct SegmentSet
 // Builds the segment list for `coils` (each at its own precision) for field
 // evaluation; precision selects whether FP32 tables are appended.
 bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err);
-// FP32 angular table of a coil at precision p (node order of the FP64 table)
-void buildPhi32(const PrecisionArgs &p, std::vector<PhiNode32> &out);
+// FP32 angular pair table of a coil at precision p: (n + 1) / 2 entries, entry i
+// for nodes i and n-1-i of the FP64 table in its reference order
+void buildPhiPairs32(const PrecisionArgs &p, std::vector<PhiNode32> &out);
+// entry k (0 <= k < (n + 1) / 2) of that table
+PhiNode32 phiPair32(const PrecisionArgs &p, int k);
 // FP32 path's near-field box of a coil, into h.near_lo / near_hi / near_r2
 void setNearBox(const Coil &k, SegmentHeader &h);
 

@@ -3,8 +3,16 @@
 // namespaces after integrands64.cuh.
 //
 // Arithmetic.  Per point and coil the frame transform, the per-thickness-node
-// constants and the final sums are FP64; the angular loop runs in FP32 with
-// Kahan-compensated accumulation per thickness node.  The FP32 integrands are
+// constants and the final sums are FP64; the angular loop runs in FP32 over
+// mirror pairs of nodes (phi, pi - phi): each step evaluates both nodes and
+// adds w cos (f(c) - f(-c)) and w (g(c) + g(-c)) to plain FP32 accumulators.
+// The cos-weighted sums cancel far from the coil; pairing cancels them inside
+// each step, where f(c) and f(-c) agree to many digits and their difference is
+// exact, so the running sums hold only the surviving part and need no
+// compensation.  Both nodes of a pair take every quantity of the form
+// Q + b2 (1 - cos) from the same FP32 constants Q and b2 (with their own
+// 1 - cos, omc and omcm), so the rounding of Q and b2 is common to the pair
+// and drops out of the difference.  The FP32 integrands are
 // algebraic rewrites of the reference's (CalculateFieldsFast.cxx,
 // CalculateFieldsSlow.cxx) that remove every cancellation FP32 cannot afford:
 //   distance^2     D - 2 p r cos  ->  (p - r)^2 + z^2 + 2 p r (1 - cos)
@@ -20,25 +28,12 @@
 //                     reference's (p / M^2)(top L1 (O J1 + N) - bot L2 (O J2 + N)),
 //                     via N = c rho^4 - p r s^2 rho^2 and O = c rho^2 - 2 p r s^2,
 //                     without its 1/rho^4 cancellation
-// and the azimuthal tables hold w*cos exactly antisymmetric about pi/2 in FP32.
+// and the azimuthal tables hold one entry per mirror pair (PhiNode32).
 
 
-struct Kahan
-{
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x)
-    {
-        float y = x - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
-};
-
-// Runs body(k, accumulator set) over the angular nodes lane, lane + LANES, ...,
-// alternating between two independent accumulator sets so consecutive nodes do
-// not wait on each other's compensated additions.
+// Runs body(k, accumulator set) over the pair entries lane, lane + LANES, ...,
+// alternating between two independent accumulator sets so consecutive entries
+// do not wait on each other's additions (and each running sum stays short).
 template <int LANES, typename Acc, typename Body>
 __device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body body)
 {
@@ -52,17 +47,47 @@ __device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body
         body(k, a0);
 }
 
+// pair entries of a table slice holding n angular nodes
+__device__ __forceinline__ int pairEntries(int n) { return (n + 1) >> 1; }
+
+// Compensated (Kahan) running sum
+struct Kahan
+{
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x)
+    {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// Plain running sum, for callers whose error is set elsewhere (the gradient,
+// whose pair sums stay far below the FP32 path's error bar, and the
+// arrangement kernels, whose FP64 sum over the secondary's nodes averages the
+// per-node rounding)
+struct PlainSum
+{
+    float s = 0.0f;
+    __device__ __forceinline__ void add(float x) { s += x; }
+    __device__ __forceinline__ double value() const { return (double)s; }
+};
+
+template <typename S>
 struct Acc1
 {
-    Kahan v;
+    S v;
 };
+template <typename S>
 struct Acc2
 {
-    Kahan h, z;
+    S h, z;
 };
 struct Acc4
 {
-    Kahan a, b, c, d;
+    float a = 0.0f, b = 0.0f, c = 0.0f, d = 0.0f;
 };
 
 // reciprocal: MUFU estimate (within 1 ulp), no special-case handling needed
@@ -160,19 +185,27 @@ __device__ __forceinline__ float asinhMid(float u)
     return u * p;
 }
 
-// Warp-uniform choice where possible: every lane below 0.25 (far points: the
-// short series), every lane below 1 (the polynomial), otherwise per lane
-__device__ __forceinline__ float asinhFast(float u)
+// asinh(u) per lane: asinhMid up to 1, asinhLarge beyond (CUDA's asinhf past 1e18)
+__device__ __forceinline__ float asinhAny(float u)
 {
     const float au = fabsf(u);
-    const unsigned mask = __activemask();
-    if (__all_sync(mask, au < 0.25f))
-        return asinhSmall(u);
-    if (__all_sync(mask, au <= 1.0f))
-        return asinhMid(u);
     if (au <= 1.0f)
         return asinhMid(u);
     return au < 1e18f ? asinhLarge(u) : asinhf(u);
+}
+
+// asinh(u) - asinh(v) for a mirror pair.  Warp-uniform choice where possible:
+// every lane's arguments below 0.25 (far points: the short series), every
+// lane's below 1 (the polynomial), otherwise per lane
+__device__ __forceinline__ float asinhDiff(float u, float v)
+{
+    const float a = fmaxf(fabsf(u), fabsf(v));
+    const unsigned mask = __activemask();
+    if (__all_sync(mask, a < 0.25f))
+        return asinhSmall(u) - asinhSmall(v);
+    if (__all_sync(mask, a <= 1.0f))
+        return asinhMid(u) - asinhMid(v);
+    return asinhAny(u) - asinhAny(v);
 }
 
 __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame &f)
@@ -180,33 +213,39 @@ __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame 
     return f.r > h.near_lo[0] && f.r < h.near_hi[0] && f.z > h.near_lo[1] && f.z < h.near_hi[1];
 }
 
-template <int LANES>
+// S: the running-sum type of the pair accumulation (Kahan or PlainSum)
+template <int LANES, typename S = Kahan>
 __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                              const PhiNode32 *pn, const Frame &f, int lane)
 {
     double sum = 0.0;
+    const int np = pairEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
         const bool same = top * bot > 0.0;
         const float topf = (float)top, botf = (float)bot;
         const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
+        // argument of the single asinh at one node from rho^2 and the two distances^2
+        auto arg = [&](float rho2, float den1, float den2) {
+            const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
+            const float a = topf * s2, b = botf * s1;
+            const float num = same ? dDf : (a - b);
+            const float den = same ? (a + b) : rho2;
+            return num * rcpApprox(den);
+        };
         for (int j = 0; j < h.n_t; ++j)
         {
             const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * f.r);
+            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+            const float qf = (float)q, b2 = (float)b2d;
             const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            Acc1 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc1 &acc) {
+            Acc1<S> a0, a1;
+            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
                 const PhiNode32 nd = pn[k];
-                const float rho2 = fmaf(b2, nd.omc, qf);
-                const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
-                const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
-                const float a = topf * s2, b = botf * s1;
-                const float num = same ? dDf : (a - b);
-                const float den = same ? (a + b) : rho2;
-                acc.v.add(nd.wc * asinhFast(num * rcpApprox(den)));
+                const float u = arg(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2));
+                const float um = arg(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2));
+                acc.v.add(nd.wc * asinhDiff(u, um));
             });
             sum += t.y * t.x * (a0.v.value() + a1.v.value());
         }
@@ -220,11 +259,13 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
             for (int j = 0; j < h.n_t; ++j)
             {
                 const double2 t = tt[j];
-                const float qf = (float)((t.x - f.r) * (t.x - f.r) + zl * zl), b2 = (float)(2.0 * t.x * f.r);
-                Acc1 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc1 &acc) {
+                const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
+                const float qf = (float)q, b2 = (float)b2d;
+                Acc1<S> a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
                     const PhiNode32 nd = pn[k];
-                    acc.v.add(nd.wc * rsqrtNR(fmaf(b2, nd.omc, qf)));
+                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
+                    acc.v.add(nd.wc * (g - gm));
                 });
                 sum += l.y * t.y * t.x * (a0.v.value() + a1.v.value());
             }
@@ -233,12 +274,13 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
     return sum;
 }
 
-template <int LANES>
+template <int LANES, typename S = Kahan>
 __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                            const PhiNode32 *pn, const Frame &f, int lane, double &H, double &Z)
 {
     H = 0.0;
     Z = 0.0;
+    const int np = pairEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
@@ -246,27 +288,34 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
         const float topf = (float)top, botf = (float)bot;
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
         const float dDf = (float)dD;
+        // one node: hv (the H integrand over dD w c) and zv (the Z integrand over w)
+        auto node = [&](float rho2, float den1, float den2, float num, float &hv, float &zv) {
+            const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
+            const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
+            const float t1 = topf * g1, t2 = botf * g2;
+            const float X = same ? (t1 + t2) : rho2;
+            const float Y = same ? dDf * gg2 : (t1 - t2);
+            const float R = rcpApprox(s * X);
+            hv = gg2 * (X * R);
+            zv = num * Y * (s * R);
+        };
         for (int j = 0; j < h.n_t; ++j)
         {
             const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * f.r);
+            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+            const float qf = (float)q, b2 = (float)b2d;
             const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
             // p^2 - p r cos = p (p - r) + p r (1 - cos)
             const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-            Acc2 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc2 &acc) {
+            Acc2<S> a0, a1;
+            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
                 const PhiNode32 nd = pn[k];
-                const float rho2 = fmaf(b2, nd.omc, qf);
-                const float g1 = rsqrtNR(fmaf(b2, nd.omc, d1)), g2 = rsqrtNR(fmaf(b2, nd.omc, d2));
-                const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
-                const float t1 = topf * g1, t2 = botf * g2;
-                const float X = same ? (t1 + t2) : rho2;
-                const float Y = same ? dDf * gg2 : (t1 - t2);
-                const float R = rcpApprox(s * X);
-                const float num = fmaf(n1, nd.omc, n0);
-                acc.h.add(nd.wc * gg2 * (X * R));
-                acc.z.add(nd.w * num * Y * (s * R));
+                float hv, zv, hm, zm;
+                node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), fmaf(n1, nd.omc, n0), hv, zv);
+                node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), fmaf(n1, nd.omcm, n0),
+                     hm, zm);
+                acc.h.add(nd.wc * (hv - hm));
+                acc.z.add(nd.w * (zv + zm));
             });
             H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
             Z += t.y * (a0.z.value() + a1.z.value());
@@ -281,15 +330,16 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
             for (int j = 0; j < h.n_t; ++j)
             {
                 const double2 t = tt[j];
-                const float qf = (float)((t.x - f.r) * (t.x - f.r) + zl * zl), b2 = (float)(2.0 * t.x * f.r);
+                const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
+                const float qf = (float)q, b2 = (float)b2d;
                 const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-                Acc2 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc2 &acc) {
+                Acc2<S> a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
                     const PhiNode32 nd = pn[k];
-                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf));
-                    const float g3 = g * g * g;
-                    acc.z.add(nd.w * g3 * fmaf(n1, nd.omc, n0));
-                    acc.h.add(nd.wc * g3);
+                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
+                    const float g3 = g * g * g, g3m = gm * gm * gm;
+                    acc.z.add(nd.w * fmaf(g3, fmaf(n1, nd.omc, n0), g3m * fmaf(n1, nd.omcm, n0)));
+                    acc.h.add(nd.wc * (g3 - g3m));
                 });
                 const double w = l.y * t.y;
                 H += w * t.x * zl * (a0.h.value() + a1.h.value());
@@ -306,6 +356,7 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
 {
     double rphi = 0.0, rr = 0.0, rz = 0.0, zz = 0.0;
     const double r = f.r;
+    const int np = pairEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
@@ -313,42 +364,52 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
         const float topf = (float)top, botf = (float)bot, lenf = (float)(2.0 * h.half_length);
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
         const float dDf = (float)dD;
+        // one node: dg = G2 - G1, dg3 = G1^3 - G2^3, cz = T1 + Y (the RZ part
+        // multiplying cos) and kz = k (2 Y + T1) / sin2 (sin2 = (b2 / 2) sin^2 is
+        // the same for both nodes of a pair).  T1 = top G1^3 - bot G2^3 and
+        // Y = (top G1 - bot G2) / rho^2, each in its cancellation-free form for a
+        // point outside / inside the slab
+        auto node = [&](float rho2, float den1, float den2, float &dg, float &dg3, float &cz, float &kz) {
+            const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
+            const float gg = g1 * g2, s = g1 + g2;
+            const float ddgg = dDf * gg * gg;
+            dg = ddgg * rcpApprox(s);
+            dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));
+            const float g13 = g1 * g1 * g1;
+            const float T1 = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
+            const float t1 = topf * g1, t2 = botf * g2;
+            const float yn = same ? ddgg : (t1 - t2);
+            const float yd = same ? (t1 + t2) : rho2;
+            const float Y = yn * rcpApprox(yd);
+            cz = T1 + Y;
+            kz = fmaf(2.0f, Y, T1) * rcpApprox(rho2);
+        };
         for (int j = 0; j < h.n_t; ++j)
         {
             const double2 t = tt[j];
-            const double q = (t.x - r) * (t.x - r);
-            const float qf = (float)q, b2 = (float)(2.0 * t.x * r);
+            const double q = (t.x - r) * (t.x - r), b2d = 2.0 * t.x * r;
+            const float qf = (float)q, b2 = (float)b2d, hb2 = (float)(0.5 * b2d);
             const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
             const float pf = (float)t.x, rf = (float)r;
+            // (r - p cos) = (r - p) + p (1 - cos); likewise (p - r cos)
             const float rmp = (float)(r - t.x), pmr = (float)(t.x - r);
             Acc4 a0, a1;
-            forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc4 &acc) {
+            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
                 const PhiNode32 nd = pn[k];
-                const float g1 = rsqrtNR(fmaf(b2, nd.omc, d1)), g2 = rsqrtNR(fmaf(b2, nd.omc, d2));
-                const float gg = g1 * g2, s = g1 + g2;
-                const float dg = dDf * gg * gg * rcpApprox(s);       // G2 - G1
-                const float dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));  // G1^3 - G2^3
-                const float g13 = g1 * g1 * g1;
-                // T1 = top G1^3 - bot G2^3 and Y = (top G1 - bot G2) / rho^2, each in
-                // its cancellation-free form for a point outside / inside the slab
-                const float T1 = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
-                const float rho2 = fmaf(b2, nd.omc, qf);
-                const float t1 = topf * g1, t2 = botf * g2;
-                const float yn = same ? dDf * gg * gg : (t1 - t2);
-                const float yd = same ? (t1 + t2) : rho2;
-                const float Y = yn * rcpApprox(yd);
-                // k = p r sin^2 / rho^2 = (b2 / 2)(1 - c)(1 + c) / rho^2
-                const float ks = (0.5f * b2) * (nd.omc * (2.0f - nd.omc)) * rcpApprox(rho2);
-                acc.a.add(nd.wc * dg);
-                acc.b.add(nd.wc * fmaf(pf, nd.omc, rmp) * dg3);   // (r - p cos)
-                acc.d.add(nd.w * fmaf(rf, nd.omc, pmr) * dg3);    // (p - r cos)
-                acc.c.add(fmaf(nd.wc, T1 + Y, -nd.w * ks * fmaf(2.0f, Y, T1)));
+                float dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
+                node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), dg, dg3, cz, kz);
+                node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), dgm, dg3m, czm, kzm);
+                const float sin2 = hb2 * (nd.omc * nd.omcm);  // p r sin^2 = (b2 / 2)(1 - c)(1 + c)
+                acc.a = fmaf(nd.wc, dg - dgm, acc.a);
+                acc.b = fmaf(nd.wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
+                acc.d = fmaf(nd.w, fmaf(fmaf(rf, nd.omc, pmr), dg3, fmaf(rf, nd.omcm, pmr) * dg3m), acc.d);
+                acc.c = fmaf(nd.wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
             });
             const double w = t.y * t.x;
-            rphi += w / r * (a0.a.value() + a1.a.value());
-            rr += w * (a0.b.value() + a1.b.value());
-            zz += w * (a0.d.value() + a1.d.value());
-            rz += w * (a0.c.value() + a1.c.value());
+            rphi += w / r * ((double)a0.a + (double)a1.a);
+            rr += w * ((double)a0.b + (double)a1.b);
+            zz += w * ((double)a0.d + (double)a1.d);
+            rz += w * ((double)a0.c + (double)a1.c);
         }
     }
     else
@@ -361,29 +422,35 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
             {
                 const double2 t = tt[j];
                 const double p = t.x;
-                const float qf = (float)((p - r) * (p - r) + zl * zl), b2 = (float)(2.0 * p * r);
+                const double q = (p - r) * (p - r) + zl * zl, b2d = 2.0 * p * r;
+                const float qf = (float)q, b2 = (float)b2d;
                 const float pf = (float)p, rf = (float)r;
                 const float rmp = (float)(r - p), pmr = (float)(p - r);
                 // RZ node G^5 (p cos (2p^2 + 2r^2 - zl^2 - p r cos) - 3 p^2 r) rewritten as
                 // -p G^5 (cos D + 3 (p - r cos)(r - p cos)), D the squared distance:
                 // no cancellation where the point approaches the ring (D -> 0)
                 Acc4 a0, a1;
-                forNodes<LANES>(h.n_phi, lane, a0, a1, [&](int k, Acc4 &acc) {
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
                     const PhiNode32 nd = pn[k];
-                    const float den = fmaf(b2, nd.omc, qf);
-                    const float gq = rsqrtNR(den);
+                    const float den = fmaf(b2, nd.omc, qf), denm = fmaf(b2, nd.omcm, qf);
+                    const float c = 0.5f * (nd.omcm - nd.omc);  // cos; the mirror's is -c
+                    const float gq = rsqrtNR(den), gqm = rsqrtNR(denm);
                     const float g3 = gq * gq * gq, g5 = g3 * gq * gq;
+                    const float g3m = gqm * gqm * gqm, g5m = g3m * gqm * gqm;
                     const float rpc = fmaf(pf, nd.omc, rmp), prc = fmaf(rf, nd.omc, pmr);
-                    acc.a.add(nd.wc * g3);
-                    acc.b.add(nd.wc * g5 * rpc);
-                    acc.d.add(nd.w * g5 * prc);
-                    acc.c.add(nd.w * g5 * fmaf(nd.c, den, 3.0f * prc * rpc));
+                    const float rpcm = fmaf(pf, nd.omcm, rmp), prcm = fmaf(rf, nd.omcm, pmr);
+                    acc.a = fmaf(nd.wc, g3 - g3m, acc.a);
+                    acc.b = fmaf(nd.wc, fmaf(g5, rpc, -g5m * rpcm), acc.b);
+                    acc.d = fmaf(nd.w, fmaf(g5, prc, g5m * prcm), acc.d);
+                    acc.c = fmaf(nd.w,
+                                 fmaf(g5, fmaf(c, den, 3.0f * prc * rpc), g5m * fmaf(-c, denm, 3.0f * prcm * rpcm)),
+                                 acc.c);
                 });
                 const double w = l.y * t.y;
-                rphi += w * p * zl / r * (a0.a.value() + a1.a.value());
-                rr += -3.0 * w * p * zl * (a0.b.value() + a1.b.value());
-                zz += -3.0 * w * p * zl * (a0.d.value() + a1.d.value());
-                rz += -w * p * (a0.c.value() + a1.c.value());
+                rphi += w * p * zl / r * ((double)a0.a + (double)a1.a);
+                rr += -3.0 * w * p * zl * ((double)a0.b + (double)a1.b);
+                zz += -3.0 * w * p * zl * ((double)a0.d + (double)a1.d);
+                rz += -w * p * ((double)a0.c + (double)a1.c);
             }
         }
     }

@@ -90,7 +90,9 @@ int buildStatic(const Coil *coils, int count, int field, size_t &blobBytes, int 
         const int nphi = p.angular_blocks * p.angular_increments;
         const int headerBytes = (int)sizeof(SegmentHeader);
         const int fixedBytes = headerBytes + 16 * (nt + nl);
-        const int maxPhi = (kSegmentBytes - fixedBytes) / 32;
+        // 16 bytes per FP64 node plus 16 per FP32 mirror-pair entry; segments cut
+        // at even node counts so that no mirror pair is split
+        const int maxPhi = 2 * ((kSegmentBytes - fixedBytes) / 48);
         if (maxPhi < 1)
             return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "a coil's thickness/length node tables exceed one segment");
         const double *tx = legendreNodes(p.thickness_increments), *tw = legendreWeights(p.thickness_increments);
@@ -148,32 +150,16 @@ int buildStatic(const Coil *coils, int count, int field, size_t &blobBytes, int 
                         w.put(e, sizeof(e));
                     }
             }
+            // the FP64 table in mirror-pair order, then the pair entries it covers
             for (int j = start; j < start + cnt; ++j)
             {
-                double e[2] = {std::cos(phiOf(j)), aw[j % p.angular_increments]};
+                const int node = pairOrderNode(j, nphi);
+                double e[2] = {std::cos(phiOf(node)), aw[node % p.angular_increments]};
                 w.put(e, sizeof(e));
             }
-            for (int j = start; j < start + cnt; ++j)
+            for (int i = start / 2; i < (start + cnt + 1) / 2; ++i)
             {
-                // exactly antisymmetric cos about pi/2: the lower index of a mirror
-                // pair defines the value, the upper one takes its negation
-                const int m = nphi - 1 - j, lo = j < m ? j : m, hi = j < m ? m : j;
-                const double wl = aw[lo % p.angular_increments];
-                const double c = 0.5 * (std::cos(phiOf(lo)) - std::cos(phiOf(hi)));
-                float cf = (float)c, wcf = (float)(wl * c);
-                if (j == m)
-                    cf = wcf = 0.0f;
-                else if (j != lo)
-                {
-                    cf = -cf;
-                    wcf = -wcf;
-                }
-                const double s = std::sin(0.5 * phiOf(j));
-                PhiNode32 nd;
-                nd.wc = wcf;
-                nd.omc = (float)(2.0 * s * s);
-                nd.c = cf;
-                nd.w = (float)aw[j % p.angular_increments];
+                const PhiNode32 nd = phiPair32(p, i);
                 w.put(&nd, sizeof(nd));
             }
             d.bytes = (int)(w.used - (size_t)d.offset);

@@ -50,42 +50,40 @@ void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
 // pi/2 (node j and its mirror n-1-j), so the FP32 sum of w*cos over the nodes
 // vanishes exactly, and 1 - cos(phi) from a half-angle sine (no cancellation
 // near phi = 0).  Node order is that of the FP64 table.
-void buildPhi32(const PrecisionArgs &p, std::vector<PhiNode32> &phi32)
+PhiNode32 phiPair32(const PrecisionArgs &p, int k)
 {
     const double aBlock = kPi / p.angular_blocks;
     const double *ax = legendreNodes(p.angular_increments), *aw = legendreWeights(p.angular_increments);
     const int n = p.angular_blocks * p.angular_increments;
-    phi32.assign(n, PhiNode32{});
-    for (int j = 0; j < n; ++j)
+    auto phiOf = [&](int j) {
+        return aBlock * (j / p.angular_increments + 0.5) + (aBlock * 0.5) * ax[j % p.angular_increments];
+    };
+    const int m = n - 1 - k;
+    const double w = aw[k % p.angular_increments];
+    const double s = std::sin(0.5 * phiOf(k)), sm = std::sin(0.5 * phiOf(m));
+    PhiNode32 e;
+    e.omc = (float)(2.0 * s * s);
+    if (m == k)
     {
-        int bp = j / p.angular_increments, i = j % p.angular_increments;
-        double phi = aBlock * (bp + 0.5) + (aBlock * 0.5) * ax[i];
-        int m = n - 1 - j;  // mirror node
-        int mbp = m / p.angular_increments, mi = m % p.angular_increments;
-        double mphi = aBlock * (mbp + 0.5) + (aBlock * 0.5) * ax[mi];
-        // symmetric definition: c(j) = (cos(phi_j) - cos(phi_m)) / 2
-        double c = 0.5 * (std::cos(phi) - std::cos(mphi));
-        double s = std::sin(0.5 * phi);
-        phi32[j].c = (float)c;
-        phi32[j].w = (float)aw[i];
-        phi32[j].wc = (float)(aw[i] * c);
-        phi32[j].omc = (float)(2.0 * s * s);
+        e.omcm = e.omc;
+        e.wc = 0.0f;
+        e.w = (float)(0.5 * w);
     }
-    for (int j = 0; j < n; ++j)
+    else
     {
-        // force exact antisymmetry of the FP32 values
-        int m = n - 1 - j;
-        if (m < j)
-        {
-            phi32[j].c = -phi32[m].c;
-            phi32[j].wc = -phi32[m].wc;
-        }
-        else if (m == j)
-        {
-            phi32[j].c = 0.0f;
-            phi32[j].wc = 0.0f;
-        }
+        e.omcm = (float)(2.0 * sm * sm);
+        e.wc = (float)(w * 0.5 * (std::cos(phiOf(k)) - std::cos(phiOf(m))));
+        e.w = (float)w;
     }
+    return e;
+}
+
+void buildPhiPairs32(const PrecisionArgs &p, std::vector<PhiNode32> &pairs)
+{
+    const int n = p.angular_blocks * p.angular_increments;
+    pairs.resize((n + 1) / 2);
+    for (int k = 0; k < (n + 1) / 2; ++k)
+        pairs[k] = phiPair32(p, k);
 }
 
 // Near-field region of the FP32 path: the winding's cross-section box in
@@ -106,7 +104,6 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
     out.segs.clear();
     out.max_bytes = 0;
     const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
-    const int perPhi = fp32 ? 32 : 16;  // bytes per angular node (FP64 entry + FP32 entry)
 
     for (int ci = 0; ci < count; ++ci)
     {
@@ -165,11 +162,21 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
                 phiNodes.push_back({std::cos(blockPos + (aBlock * 0.5) * ax[i]), aw[i]});
         }
         if (fp32)
-            buildPhi32(p, phi32);
+        {
+            // FP32 mode: the FP64 table (used by the near-field pass) in mirror-pair
+            // order, so that every segment's FP64 and FP32 tables cover the same nodes
+            std::vector<Entry> paired(phiNodes.size());
+            for (size_t j = 0; j < phiNodes.size(); ++j)
+                paired[j] = phiNodes[pairOrderNode((int)j, (int)phiNodes.size())];
+            phiNodes.swap(paired);
+            buildPhiPairs32(p, phi32);
+        }
 
         const int headerBytes = (int)sizeof(SegmentHeader);
         const int fixedBytes = headerBytes + 16 * (int)(tNodes.size() + lNodes.size());
-        const int maxPhi = (kSegmentBytes - fixedBytes) / perPhi;
+        // FP32 mode: 16 bytes per FP64 node plus 16 per pair entry, and segments
+        // cut at even node counts so that no mirror pair is split
+        const int maxPhi = fp32 ? 2 * ((kSegmentBytes - fixedBytes) / 48) : (kSegmentBytes - fixedBytes) / 16;
         if (maxPhi < 1)
         {
             err = "coil " + std::to_string(ci) + ": thickness/length node tables exceed one staging segment";
@@ -206,7 +213,7 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
             appendBytes(out.blob, lNodes.data(), 16 * lNodes.size());
             appendBytes(out.blob, phiNodes.data() + start, 16 * (size_t)cnt);
             if (fp32)
-                appendBytes(out.blob, phi32.data() + start, 16 * (size_t)cnt);
+                appendBytes(out.blob, phi32.data() + start / 2, 16 * (size_t)((cnt + 1) / 2));
             d.bytes = (int)(out.blob.size() - d.offset);
             out.max_bytes = std::max(out.max_bytes, d.bytes);
             out.segs.push_back(d);
