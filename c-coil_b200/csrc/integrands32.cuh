@@ -99,15 +99,18 @@ __device__ __forceinline__ float rcpApprox(float x)
     return y;
 }
 
-// reciprocal square root: the MUFU estimate (relative error below 2^-22.9); a
-// Newton-Raphson step (CCOIL_RSQRT_NEWTON=1) did not change the measured error
-// of the sums, which is set by the far-field cancellation, and costs 4 FMA per call
+// reciprocal square root: the MUFU estimate (relative error below 2^-22.9),
+// flush-to-zero form (one instruction; every argument here is a positive
+// normal number, a squared distance or 1 + u^2); a Newton-Raphson step
+// (CCOIL_RSQRT_NEWTON=1) did not change the measured error of the sums, which
+// is set by the far-field cancellation, and costs 4 FMA per call
 #ifndef CCOIL_RSQRT_NEWTON
 #define CCOIL_RSQRT_NEWTON 0
 #endif
 __device__ __forceinline__ float rsqrtNR(float x)
 {
-    float y = rsqrtf(x);
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
 #if CCOIL_RSQRT_NEWTON
     float e = fmaf(-x * y, y, 1.0f);
     y = fmaf(0.5f * y, e, y);
