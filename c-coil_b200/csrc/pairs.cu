@@ -284,6 +284,13 @@ __device__ __forceinline__ void transformDerivatives(double yA, double zA, doubl
 #ifndef CCOIL_PAIR_MIN_BLOCKS
 #define CCOIL_PAIR_MIN_BLOCKS 6
 #endif
+// the same for the FP32 variants (M and F/T): 9 (56 registers) measured best
+// on B200 against 6, 7, 8 and 10 (M 70.3 ms at 2^18 arrangements against
+// 78.3, 73.7, 71.8 and 73.1; F/T flat at 48 ms); the FP32 kernel's lanes wait
+// on fixed-latency chains, which more resident warps hide
+#ifndef CCOIL_PAIR32_MIN_BLOCKS
+#define CCOIL_PAIR32_MIN_BLOCKS 9
+#endif
 // largest single-primary blob staged in shared memory (0 turns staging off)
 #ifndef CCOIL_PAIR_STAGE_MAX_BYTES
 #define CCOIL_PAIR_STAGE_MAX_BYTES (48 * 1024)
@@ -354,7 +361,7 @@ __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *t
 // work runs on full warps instead of dragging whole mixed iterations along;
 // the secondary-node sums and the cross-lane reduction stay FP64.
 template <int QTY, bool FP32>
-__global__ void __launch_bounds__(128, CCOIL_PAIR_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
                  const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
                  double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes,
