@@ -52,10 +52,24 @@ struct NearPair
     int segment;
 };
 
-// minimum resident CTAs per SM requested from the register allocator
-// CTAs per SM the register allocation targets: 6 for the vector potential
-// (fewer live values), 5 for B and the gradient (measured best on B200)
-constexpr int fp32MinBlocks(int field) { return field == CCOIL_FIELD_B || field == CCOIL_FIELD_G ? 5 : 6; }
+// CTAs per SM the register allocation targets, measured best on B200 over
+// 4-8 (2^20 points, 128-coil group): 6 for the vector potential, 5 for B,
+// 4 for the gradient (126 registers, no spills: 3.5 % faster than 5 CTAs
+// with 96 registers and spills; 3 CTAs was no faster)
+#ifndef CCOIL_FP32_MIN_BLOCKS_A
+#define CCOIL_FP32_MIN_BLOCKS_A 6
+#endif
+#ifndef CCOIL_FP32_MIN_BLOCKS_B
+#define CCOIL_FP32_MIN_BLOCKS_B 5
+#endif
+#ifndef CCOIL_FP32_MIN_BLOCKS_G
+#define CCOIL_FP32_MIN_BLOCKS_G 4
+#endif
+constexpr int fp32MinBlocks(int field)
+{
+    return field == CCOIL_FIELD_B ? CCOIL_FP32_MIN_BLOCKS_B
+                                  : (field == CCOIL_FIELD_G ? CCOIL_FP32_MIN_BLOCKS_G : CCOIL_FP32_MIN_BLOCKS_A);
+}
 // 1: segments are staged into shared memory by bulk copies (double-buffered,
 // one CTA barrier per segment); 0 (default, 1.9x faster on B200): each warp
 // reads the segment tables from global memory through L1 -- the same table
