@@ -50,6 +50,40 @@ __device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body
 // pair entries of a table slice holding n angular nodes
 __device__ __forceinline__ int pairEntries(int n) { return (n + 1) >> 1; }
 
+// Fast method: whether a point lies outside the coil's length slab (|z| > b/2)
+// picks between two cancellation-free forms of each integrand.  When every
+// active lane agrees the warp runs a loop with that form only (SLAB 1: all
+// outside, 2: all inside); otherwise each lane selects (SLAB 0).
+template <int V>
+struct SlabTag
+{
+    static constexpr int value = V;
+};
+// UNIFORM false: always the per-lane form (B, measured no faster with the
+// branches, and the arrangement kernels, whose out-of-line quadrature measured
+// 35 % slower with the three loop copies).
+template <bool UNIFORM, typename Loop>
+__device__ __forceinline__ void bySlab(bool outside, Loop loop)
+{
+    if (!UNIFORM)
+    {
+        loop(SlabTag<0>{});
+        return;
+    }
+    const unsigned mask = __activemask();
+    if (__all_sync(mask, outside))
+        loop(SlabTag<1>{});
+    else if (__all_sync(mask, !outside))
+        loop(SlabTag<2>{});
+    else
+        loop(SlabTag<0>{});
+}
+template <int SLAB>
+__device__ __forceinline__ bool slabOutside(bool perLane)
+{
+    return SLAB == 1 ? true : (SLAB == 2 ? false : perLane);
+}
+
 // Compensated (Kahan) running sum
 struct Kahan
 {
@@ -216,8 +250,9 @@ __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame 
     return f.r > h.near_lo[0] && f.r < h.near_hi[0] && f.z > h.near_lo[1] && f.z < h.near_hi[1];
 }
 
-// S: the running-sum type of the pair accumulation (Kahan or PlainSum)
-template <int LANES, typename S = Kahan>
+// S: the running-sum type of the pair accumulation (Kahan or PlainSum);
+// UNIFORM: warp-uniform slab branches (bySlab)
+template <int LANES, typename S = Kahan, bool UNIFORM = true>
 __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                              const PhiNode32 *pn, const Frame &f, int lane)
 {
@@ -229,29 +264,32 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
         const bool same = top * bot > 0.0;
         const float topf = (float)top, botf = (float)bot;
         const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
-        // argument of the single asinh at one node from rho^2 and the two distances^2
-        auto arg = [&](float rho2, float den1, float den2) {
-            const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
-            const float a = topf * s2, b = botf * s1;
-            const float num = same ? dDf : (a - b);
-            const float den = same ? (a + b) : rho2;
-            return num * rcpApprox(den);
-        };
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
-            const float qf = (float)q, b2 = (float)b2d;
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            Acc1<S> a0, a1;
-            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
-                const PhiNode32 nd = pn[k];
-                const float u = arg(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2));
-                const float um = arg(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2));
-                acc.v.add(nd.wc * asinhDiff(u, um));
-            });
-            sum += t.y * t.x * (a0.v.value() + a1.v.value());
-        }
+        bySlab<UNIFORM>(same, [&](auto slab) {
+            const bool outside = slabOutside<decltype(slab)::value>(same);
+            // argument of the single asinh at one node from rho^2 and the two distances^2
+            auto arg = [&](float rho2, float den1, float den2) {
+                const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
+                const float a = topf * s2, b = botf * s1;
+                const float num = outside ? dDf : (a - b);
+                const float den = outside ? (a + b) : rho2;
+                return num * rcpApprox(den);
+            };
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+                const float qf = (float)q, b2 = (float)b2d;
+                const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+                Acc1<S> a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
+                    const PhiNode32 nd = pn[k];
+                    const float u = arg(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2));
+                    const float um = arg(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2));
+                    acc.v.add(nd.wc * asinhDiff(u, um));
+                });
+                sum += t.y * t.x * (a0.v.value() + a1.v.value());
+            }
+        });
     }
     else
     {
@@ -291,38 +329,42 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
         const float topf = (float)top, botf = (float)bot;
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
         const float dDf = (float)dD;
-        // one node: hv (the H integrand over dD w c) and zv (the Z integrand over w)
-        auto node = [&](float rho2, float den1, float den2, float num, float &hv, float &zv) {
-            const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
-            const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
-            const float t1 = topf * g1, t2 = botf * g2;
-            const float X = same ? (t1 + t2) : rho2;
-            const float Y = same ? dDf * gg2 : (t1 - t2);
-            const float R = rcpApprox(s * X);
-            hv = gg2 * (X * R);
-            zv = num * Y * (s * R);
-        };
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
-            const float qf = (float)q, b2 = (float)b2d;
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            // p^2 - p r cos = p (p - r) + p r (1 - cos)
-            const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-            Acc2<S> a0, a1;
-            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
-                const PhiNode32 nd = pn[k];
-                float hv, zv, hm, zm;
-                node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), fmaf(n1, nd.omc, n0), hv, zv);
-                node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), fmaf(n1, nd.omcm, n0),
-                     hm, zm);
-                acc.h.add(nd.wc * (hv - hm));
-                acc.z.add(nd.w * (zv + zm));
-            });
-            H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
-            Z += t.y * (a0.z.value() + a1.z.value());
-        }
+        bySlab<false>(same, [&](auto slab) {  // per lane: branches measured no faster for B
+            const bool outside = slabOutside<decltype(slab)::value>(same);
+            // one node: hv (the H integrand over dD w c) and zv (the Z integrand over w)
+            auto node = [&](float rho2, float den1, float den2, float num, float &hv, float &zv) {
+                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
+                const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
+                const float t1 = topf * g1, t2 = botf * g2;
+                const float X = outside ? (t1 + t2) : rho2;
+                const float Y = outside ? dDf * gg2 : (t1 - t2);
+                const float R = rcpApprox(s * X);
+                hv = gg2 * (X * R);
+                zv = num * Y * (s * R);
+            };
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+                const float qf = (float)q, b2 = (float)b2d;
+                const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+                // p^2 - p r cos = p (p - r) + p r (1 - cos)
+                const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
+                Acc2<S> a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
+                    const PhiNode32 nd = pn[k];
+                    float hv, zv, hm, zm;
+                    node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), fmaf(n1, nd.omc, n0), hv,
+                         zv);
+                    node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), fmaf(n1, nd.omcm, n0),
+                         hm, zm);
+                    acc.h.add(nd.wc * (hv - hm));
+                    acc.z.add(nd.w * (zv + zm));
+                });
+                H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
+                Z += t.y * (a0.z.value() + a1.z.value());
+            }
+        });
     }
     else
     {
@@ -367,53 +409,56 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
         const float topf = (float)top, botf = (float)bot, lenf = (float)(2.0 * h.half_length);
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
         const float dDf = (float)dD;
-        // one node: dg = G2 - G1, dg3 = G1^3 - G2^3, cz = T1 + Y (the RZ part
-        // multiplying cos) and kz = k (2 Y + T1) / sin2 (sin2 = (b2 / 2) sin^2 is
-        // the same for both nodes of a pair).  T1 = top G1^3 - bot G2^3 and
-        // Y = (top G1 - bot G2) / rho^2, each in its cancellation-free form for a
-        // point outside / inside the slab
-        auto node = [&](float rho2, float den1, float den2, float &dg, float &dg3, float &cz, float &kz) {
-            const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
-            const float gg = g1 * g2, s = g1 + g2;
-            const float ddgg = dDf * gg * gg;
-            dg = ddgg * rcpApprox(s);
-            dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));
-            const float g13 = g1 * g1 * g1;
-            const float T1 = same ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
-            const float t1 = topf * g1, t2 = botf * g2;
-            const float yn = same ? ddgg : (t1 - t2);
-            const float yd = same ? (t1 + t2) : rho2;
-            const float Y = yn * rcpApprox(yd);
-            cz = T1 + Y;
-            kz = fmaf(2.0f, Y, T1) * rcpApprox(rho2);
-        };
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - r) * (t.x - r), b2d = 2.0 * t.x * r;
-            const float qf = (float)q, b2 = (float)b2d, hb2 = (float)(0.5 * b2d);
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            const float pf = (float)t.x, rf = (float)r;
-            // (r - p cos) = (r - p) + p (1 - cos); likewise (p - r cos)
-            const float rmp = (float)(r - t.x), pmr = (float)(t.x - r);
-            Acc4 a0, a1;
-            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
-                const PhiNode32 nd = pn[k];
-                float dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
-                node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), dg, dg3, cz, kz);
-                node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), dgm, dg3m, czm, kzm);
-                const float sin2 = hb2 * (nd.omc * nd.omcm);  // p r sin^2 = (b2 / 2)(1 - c)(1 + c)
-                acc.a = fmaf(nd.wc, dg - dgm, acc.a);
-                acc.b = fmaf(nd.wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
-                acc.d = fmaf(nd.w, fmaf(fmaf(rf, nd.omc, pmr), dg3, fmaf(rf, nd.omcm, pmr) * dg3m), acc.d);
-                acc.c = fmaf(nd.wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
-            });
-            const double w = t.y * t.x;
-            rphi += w / r * ((double)a0.a + (double)a1.a);
-            rr += w * ((double)a0.b + (double)a1.b);
-            zz += w * ((double)a0.d + (double)a1.d);
-            rz += w * ((double)a0.c + (double)a1.c);
-        }
+        bySlab<true>(same, [&](auto slab) {
+            const bool outside = slabOutside<decltype(slab)::value>(same);
+            // one node: dg = G2 - G1, dg3 = G1^3 - G2^3, cz = T1 + Y (the RZ part
+            // multiplying cos) and kz = k (2 Y + T1) / sin2 (sin2 = (b2 / 2) sin^2 is
+            // the same for both nodes of a pair).  T1 = top G1^3 - bot G2^3 and
+            // Y = (top G1 - bot G2) / rho^2, each in its cancellation-free form for a
+            // point outside / inside the slab
+            auto node = [&](float rho2, float den1, float den2, float &dg, float &dg3, float &cz, float &kz) {
+                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
+                const float gg = g1 * g2, s = g1 + g2;
+                const float ddgg = dDf * gg * gg;
+                dg = ddgg * rcpApprox(s);
+                dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));
+                const float g13 = g1 * g1 * g1;
+                const float T1 = outside ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
+                const float t1 = topf * g1, t2 = botf * g2;
+                const float yn = outside ? ddgg : (t1 - t2);
+                const float yd = outside ? (t1 + t2) : rho2;
+                const float Y = yn * rcpApprox(yd);
+                cz = T1 + Y;
+                kz = fmaf(2.0f, Y, T1) * rcpApprox(rho2);
+            };
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - r) * (t.x - r), b2d = 2.0 * t.x * r;
+                const float qf = (float)q, b2 = (float)b2d, hb2 = (float)(0.5 * b2d);
+                const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+                const float pf = (float)t.x, rf = (float)r;
+                // (r - p cos) = (r - p) + p (1 - cos); likewise (p - r cos)
+                const float rmp = (float)(r - t.x), pmr = (float)(t.x - r);
+                Acc4 a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
+                    const PhiNode32 nd = pn[k];
+                    float dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
+                    node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), dg, dg3, cz, kz);
+                    node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), dgm, dg3m, czm, kzm);
+                    const float sin2 = hb2 * (nd.omc * nd.omcm);  // p r sin^2 = (b2 / 2)(1 - c)(1 + c)
+                    acc.a = fmaf(nd.wc, dg - dgm, acc.a);
+                    acc.b = fmaf(nd.wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
+                    acc.d = fmaf(nd.w, fmaf(fmaf(rf, nd.omc, pmr), dg3, fmaf(rf, nd.omcm, pmr) * dg3m), acc.d);
+                    acc.c = fmaf(nd.wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
+                });
+                const double w = t.y * t.x;
+                rphi += w / r * ((double)a0.a + (double)a1.a);
+                rr += w * ((double)a0.b + (double)a1.b);
+                zz += w * ((double)a0.d + (double)a1.d);
+                rz += w * ((double)a0.c + (double)a1.c);
+            }
+        });
     }
     else
     {
