@@ -122,3 +122,37 @@ def test_gradient_across_precision_factors(ccoil, pf):
     f64, f32 = (evaluate(ccoil, coils, pts, 3, m) for m in modes(ccoil))
     e = rel_err(f32, f64)[~gradient_band(rows, pts)]
     assert np.median(e) < 1e-7 and e.max() < 1e-5, (pf, np.median(e), e.max())
+
+
+@pytest.mark.parametrize("angular", [(1, 3), (1, 7), (3, 11), (26, 99), (27, 99)])
+def test_mirror_pair_tables(ccoil, angular):
+    """The FP32 path evaluates angular nodes in mirror pairs (phi, pi - phi).  Odd
+    node counts leave a middle node of its own (3, 7, 33, 2673 nodes), and long
+    tables span several segments that must be cut between pairs (2574 and 2673
+    nodes): every coil type and field still agrees with the FP64 path.  A node
+    left out, counted twice or weighted wrongly shows up at 1e-3 or more; the
+    bars sit below that but above the rounding of tables this short, where the
+    far-field cancellation rests on one or two pairs instead of averaging over
+    many (single-pair rounding reaches ~2e-5 at 3 nodes)."""
+    from ccoil_b200 import workloads
+    blocks, increments = angular
+    prec = ccoil.PrecisionArguments(blocks, 1, 1, increments, 6, 5)
+    # {R, a, b, N, I, f, x, y, z, yAngle, zAngle}: RECTANGULAR, THIN, FLAT, FILAMENT
+    rows = np.array([[0.1, 0.05, 0.08, 100, 1.0, 50.0, 0.05, -0.02, 0.1, 0.7, 0.0],
+                     [0.12, 0.0, 0.1, 100, 1.0, 50.0, 0.0, 0.0, 0.0, 0.0, 1.1],
+                     [0.08, 0.04, 0.0, 100, 1.0, 50.0, 0.0, 0.0, 0.0, 2.0, 0.0],
+                     [0.1, 0.0, 0.0, 100, 1.0, 50.0, -0.1, 0.0, 0.05, 0.0, 0.0]])
+    pts = workloads.points_cube(2048, seed=31, half=0.5)
+    for row, coil in zip(rows, workloads.coils_from_rows(rows, 5.0)):
+        for field in (0, 1, 3):
+            res = []
+            for mode in modes(ccoil):
+                plan = ccoil.FieldPlan([coil.struct(prec)], field, mode)
+                try:
+                    res.append(plan(pts))
+                finally:
+                    plan.close()
+            e = rel_err(res[1], res[0])
+            if field == 3:
+                e = e[~gradient_band(row[None, :], pts)]
+            assert np.median(e) < 1e-6 and e.max() < 1e-4, (angular, row[:3], field, np.median(e), e.max())
