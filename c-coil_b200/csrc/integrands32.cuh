@@ -231,16 +231,13 @@ __device__ __forceinline__ float asinhAny(float u)
     return au < 1e18f ? asinhLarge(u) : asinhf(u);
 }
 
-// asinh(u) - asinh(v) for a mirror pair.  Warp-uniform choice where possible:
-// every lane's arguments below 0.25 (far points: the short series), every
-// lane's below 1 (the polynomial), otherwise per lane
-__device__ __forceinline__ float asinhDiff(float u, float v)
+// asinh(u) - asinh(v) for a mirror pair in a tier the warp chose beforehand:
+// 0 every lane's arguments below 0.25, 1 below 1, 2 per lane
+__device__ __forceinline__ float asinhDiffTier(float u, float v, int tier)
 {
-    const float a = fmaxf(fabsf(u), fabsf(v));
-    const unsigned mask = __activemask();
-    if (__all_sync(mask, a < 0.25f))
+    if (tier == 0)
         return asinhSmall(u) - asinhSmall(v);
-    if (__all_sync(mask, a <= 1.0f))
+    if (tier == 1)
         return asinhMid(u) - asinhMid(v);
     return asinhAny(u) - asinhAny(v);
 }
@@ -280,12 +277,18 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
                 const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
                 const float qf = (float)q, b2 = (float)b2d;
                 const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+                // |u| decreases with 1 - cos on either side of the slab, so its value
+                // at phi = 0 bounds every node of this thickness node: one warp vote
+                // picks the asinh form for all of them
+                const float u0 = fabsf(arg(qf, d1, d2));
+                const unsigned mask = __activemask();
+                const int tier = __all_sync(mask, u0 < 0.25f) ? 0 : (__all_sync(mask, u0 <= 1.0f) ? 1 : 2);
                 Acc1<S> a0, a1;
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
                     const PhiNode32 nd = pn[k];
                     const float u = arg(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2));
                     const float um = arg(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2));
-                    acc.v.add(nd.wc * asinhDiff(u, um));
+                    acc.v.add(nd.wc * asinhDiffTier(u, um, tier));
                 });
                 sum += t.y * t.x * (a0.v.value() + a1.v.value());
             }
