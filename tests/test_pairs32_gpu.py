@@ -49,6 +49,23 @@ def test_seeded_arrangements(ccoil):
     check_ft(a, b)
 
 
+@pytest.mark.parametrize("pf", [1.0, 4.0, 7.0])
+def test_odd_primary_angular_counts(ccoil, pf):
+    """At these PrecisionFactors the primary's angular node count is odd (17, 29,
+    49), so its FP32 mirror-pair table ends in a middle node of its own."""
+    from ccoil_b200 import workloads
+    prim_row, sec_row, ppos, spos, py, pz, sy, sz = workloads.pair_config(arrangements=1024, seed=19,
+                                                                          coaxial_fraction=0.05)
+    prim, sec = coils(ccoil, prim_row, sec_row, pf=pf)
+    pp, _ = ccoil.Coil._pair_args(prim, sec, pf)
+    assert (pp.angular_blocks * pp.angular_increments) % 2 == 1
+    args = (prim, sec, ppos, spos, py, pz, sy, sz, ccoil.PrecisionFactor(pf))
+    a, b = both(ccoil, ccoil.Coil.compute_all_mutual_inductance_arrangements, *args)
+    check_m(a, b)
+    a, b = both(ccoil, ccoil.Coil.compute_all_force_torque_arrangements, *args)
+    check_ft(a, b)
+
+
 def test_slow_method_primary(ccoil):
     """FLAT primary (slow method, length x thickness x angle) and FILAMENT secondary."""
     from ccoil_b200 import workloads
