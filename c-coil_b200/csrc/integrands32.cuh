@@ -5,11 +5,13 @@
 // Arithmetic.  Per point and coil the frame transform, the per-thickness-node
 // constants and the final sums are FP64; the angular loop runs in FP32 over
 // mirror pairs of nodes (phi, pi - phi): each step evaluates both nodes and
-// adds w cos (f(c) - f(-c)) and w (g(c) + g(-c)) to plain FP32 accumulators.
+// adds w cos (f(c) - f(-c)) and w (g(c) + g(-c)) to FP32 running sums.
 // The cos-weighted sums cancel far from the coil; pairing cancels them inside
 // each step, where f(c) and f(-c) agree to many digits and their difference is
-// exact, so the running sums hold only the surviving part and need no
-// compensation.  Both nodes of a pair take every quantity of the form
+// exact, so the running sums hold only the surviving part.  The vector
+// potential and the field still compensate their sums (Kahan: it halves their
+// 99th-percentile error); the gradient and the arrangement kernels add plainly
+// (their error is set elsewhere).  Both nodes of a pair take every quantity of the form
 // Q + b2 (1 - cos) from the same FP32 constants Q and b2 (with their own
 // 1 - cos, omc and omcm), so the rounding of Q and b2 is common to the pair
 // and drops out of the difference.  The FP32 integrands are

@@ -10,8 +10,9 @@
 //               src/CoilGroup/MInductance/ComputeMInductance.cxx:4-20,
 //               src/CoilGroup/ForceAndTorque/ComputeForce.cxx:4-28
 // The secondary is a cloud of nodes (length x thickness x azimuth); at each
-// node the primary's A (for M) or B (for F/T) is the full FP64 field quadrature
-// of integrands64.cuh.
+// node the primary's A (for M) or B (for F/T) is the full field quadrature:
+// FP64 (integrands64.cuh), or FP32-compensated (integrands32.cuh) with FP64
+// for secondary nodes in the primary's near-field box.
 //
 // Mapping.  One warp per arrangement (grid-stride); the 32 lanes split the
 // secondary's nodes, each lane evaluates the primary's whole quadrature at its
