@@ -117,9 +117,13 @@ __device__ __forceinline__ void batchItemLanes(const BatchItem &I, const unsigne
 #define CCOIL_BATCH32_MIN_BLOCKS 4
 #endif
 
+constexpr int batchMinBlocks(int prec)
+{
+    return prec == CCOIL_PRECISION_FP64 ? CCOIL_BATCH_MIN_BLOCKS : CCOIL_BATCH32_MIN_BLOCKS;
+}
+
 template <int PREC>
-__global__ void __launch_bounds__(128, PREC == CCOIL_PRECISION_FP64 ? CCOIL_BATCH_MIN_BLOCKS
-                                                                    : CCOIL_BATCH32_MIN_BLOCKS) batchKernel(const unsigned char *__restrict__ blob,
+__global__ void __launch_bounds__(128, batchMinBlocks(PREC)) batchKernel(const unsigned char *__restrict__ blob,
                                                       const SegmentDesc *__restrict__ segs,
                                                       const BatchItem *__restrict__ items, int nitems,
                                                       unsigned *__restrict__ next, const double *__restrict__ points,
