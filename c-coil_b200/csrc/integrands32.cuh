@@ -480,13 +480,13 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 const float pf = (float)p, rf = (float)r;
                 const float rmp = (float)(r - p), pmr = (float)(p - r);
                 // RZ node G^5 (p cos (2p^2 + 2r^2 - zl^2 - p r cos) - 3 p^2 r) rewritten as
-                // -p G^5 (cos D + 3 (p - r cos)(r - p cos)), D the squared distance:
-                // no cancellation where the point approaches the ring (D -> 0)
+                // -p (cos G^3 + 3 G^5 (p - r cos)(r - p cos)) (G^5 D = G^3, D the squared
+                // distance): its cos G^3 sum is the RPhi sum, so only the second sum is
+                // accumulated, and the two are combined in FP64 after the loop
                 Acc4 a0, a1;
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
                     const PhiNode32 nd = pn[k];
                     const float den = fmaf(b2, nd.omc, qf), denm = fmaf(b2, nd.omcm, qf);
-                    const float c = 0.5f * (nd.omcm - nd.omc);  // cos; the mirror's is -c
                     const float gq = rsqrtNR(den), gqm = rsqrtNR(denm);
                     const float g3 = gq * gq * gq, g5 = g3 * gq * gq;
                     const float g3m = gqm * gqm * gqm, g5m = g3m * gqm * gqm;
@@ -495,15 +495,13 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                     acc.a = fmaf(nd.wc, g3 - g3m, acc.a);
                     acc.b = fmaf(nd.wc, fmaf(g5, rpc, -g5m * rpcm), acc.b);
                     acc.d = fmaf(nd.w, fmaf(g5, prc, g5m * prcm), acc.d);
-                    acc.c = fmaf(nd.w,
-                                 fmaf(g5, fmaf(c, den, 3.0f * prc * rpc), g5m * fmaf(-c, denm, 3.0f * prcm * rpcm)),
-                                 acc.c);
+                    acc.c = fmaf(nd.w, fmaf(g5 * prc, rpc, g5m * prcm * rpcm), acc.c);
                 });
-                const double w = l.y * t.y;
-                rphi += w * p * zl / r * ((double)a0.a + (double)a1.a);
+                const double w = l.y * t.y, ca = (double)a0.a + (double)a1.a;
+                rphi += w * p * zl / r * ca;
                 rr += -3.0 * w * p * zl * ((double)a0.b + (double)a1.b);
                 zz += -3.0 * w * p * zl * ((double)a0.d + (double)a1.d);
-                rz += -w * p * ((double)a0.c + (double)a1.c);
+                rz += -w * p * (ca + 3.0 * ((double)a0.c + (double)a1.c));
             }
         }
     }
