@@ -1,7 +1,7 @@
 // ccoil_fields_fp32c_static: the FP32-compensated field evaluation for callers
-// that cannot allocate device memory -- code running while a CUDA graph is being
-// captured, plugins living inside a host application that owns every device
-// allocation, or real-time loops where an allocation could stall.  It allocates
+// that cannot allocate device memory -- plugins living inside a host
+// application that owns (and budgets) every device allocation, or real-time
+// loops where an allocation could stall.  It allocates
 // nothing: the scratch the kernel needs (the coil node tables, the segment list,
 // the near-field work list and its counter) lives in one file-scope __device__
 // array of fixed size, and the node tables are built on the host into a fixed

@@ -307,9 +307,10 @@ int ccoil_b_field_adjoint(const double *params, const ccoil_precision_args_t *pr
 long long ccoil_timeout_count(void);
 
 /* FP32_COMPENSATED field evaluation that allocates nothing.  No counterpart in
- * the reference.  For callers that cannot allocate device memory: code that
- * runs while a CUDA graph is being captured, plugins inside a host program
- * that owns every device allocation, real-time loops that must not stall.
+ * the reference.  For callers that cannot allocate device memory: plugins
+ * inside a host program that owns every device allocation (and budgets the
+ * device memory itself), real-time loops that must not stall on an
+ * allocation.
  * Same arguments and results as ccoil_compute_fields with precision
  * FP32_COMPENSATED, except that `points` and `out` must be device pointers
  * and the call is asynchronous on `stream`.

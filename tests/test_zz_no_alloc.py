@@ -1,8 +1,8 @@
 """The allocation-free entry point (ccoil_fields_fp32c_static) against the
 plan-based FP32_COMPENSATED path, through the C-ABI, on two calls in a row.
 
-It serves callers that cannot allocate device memory (graph capture, host
-programs that own every allocation); its scratch is a fixed array in device
+It serves callers that cannot allocate device memory (host programs that own
+every device allocation, real-time loops that must not stall on one); its scratch is a fixed array in device
 memory shared by all calls, so the second call also checks that the state the
 first one left behind does not leak into the result."""
 import ctypes
