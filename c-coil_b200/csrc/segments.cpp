@@ -46,10 +46,12 @@ void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
 }
 } // namespace
 
-// The FP32 angular table: cos(phi) built to be exactly antisymmetric about
-// pi/2 (node j and its mirror n-1-j), so the FP32 sum of w*cos over the nodes
-// vanishes exactly, and 1 - cos(phi) from a half-angle sine (no cancellation
-// near phi = 0).  Node order is that of the FP64 table.
+// Entry k of the FP32 angular pair table: node k of the FP64 table (in the
+// reference's order) and its mirror n-1-k.  The weighted cosine takes the
+// symmetric definition (cos(phi_k) - cos(phi_m)) / 2, so the mirror's is its
+// exact negation; both nodes' 1 - cos come from half-angle sines (no
+// cancellation near phi = 0 or pi); an odd table's middle node is an entry of
+// its own with half its weight.
 PhiNode32 phiPair32(const PrecisionArgs &p, int k)
 {
     const double aBlock = kPi / p.angular_blocks;
