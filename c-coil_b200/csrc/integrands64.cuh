@@ -8,6 +8,8 @@
 //   A/B/G slow  src/Coil/Fields/CalculateFieldsSlow.cxx:13-265
 //   Cartesian wrappers  src/Coil/Fields/CalculateFieldsMethods.cxx:6-84
 
+#include "log64.cuh"
+
 struct Frame
 {
     double z, r, cphi, sphi;
@@ -83,7 +85,7 @@ __device__ __forceinline__ double segmentA64(const SegmentHeader &h, const doubl
                 const double g = dvd(1.0, sqr(sub(cB, mul(cA, q.x))));
                 const double d1 = mul(top, g), d2 = mul(bot, g);
                 const double e1 = sqr(add(mul(d1, d1), 1.0)), e2 = sqr(add(mul(d2, d2), 1.0));
-                const double lg = log(dvd(add(e1, d1), add(e2, d2)));
+                const double lg = log64(dvd(add(e1, d1), add(e2, d2)));
                 part += mul(mul(q.y, q.x), lg);
             }
             sum += mul(mul(t.y, t.x), part);

@@ -11,6 +11,8 @@
 
 #include <cuda_runtime.h>
 
+#include "log64.cuh"
+
 namespace ccoil
 {
 namespace
@@ -95,7 +97,7 @@ __global__ void op64Kernel(double *sink, int iters)
             else if (OP == 1)
                 v[i] = __dadd_rn(__dsqrt_rn(v[i]), 1.0);
             else
-                v[i] = __dadd_rn(log(v[i]), 2.0);
+                v[i] = __dadd_rn(log64(v[i]), 2.0);  // the integrands' logarithm
         }
     double s = 0.0;
 #pragma unroll
@@ -103,6 +105,12 @@ __global__ void op64Kernel(double *sink, int iters)
         s += v[i];
     if (s == 1.2345)
         sink[0] = s;
+}
+
+__global__ void log64Kernel(const double *__restrict__ x, double *__restrict__ out, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = log64(x[i]);
 }
 
 template <typename Launch>
@@ -198,4 +206,24 @@ extern "C" int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops
     *fp32_tflops = 2.0 * lanes * it32 / (ms32 * 1e-3) / 1e12;
     *mufu_tops = lanes * itMufu / (msMu * 1e-3) / 1e12;
     return CCOIL_OK;
+}
+
+extern "C" int ccoil_eval_log64(const double *x, double *out, long long n, void *stream)
+{
+    if (n < 0 || (n > 0 && (!x || !out)))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "null input or output, or n < 0");
+    if (n == 0)
+        return CCOIL_OK;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess)
+        return fail(CCOIL_ERR_NO_DEVICE, cudaGetErrorString(e));
+    const long long want = (n + 255) / 256, cap = 8LL * sms;
+    log64Kernel<<<(unsigned)(want < cap ? want : cap), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, out, n);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? CCOIL_OK : fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
 }

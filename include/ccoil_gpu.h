@@ -334,11 +334,19 @@ int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops, double *m
 
 /* Diagnostic with no counterpart in the reference: measured rates (operations
  * per second, whole device) of rates[0] FP64-pipe instructions (FMA),
- * rates[1] __ddiv_rn, rates[2] __dsqrt_rn, rates[3] double log,
+ * rates[1] __ddiv_rn, rates[2] __dsqrt_rn, rates[3] the FP64 integrands'
+ * logarithm (see ccoil_eval_log64),
  * rates[4] FP32 FMA instructions, rates[5] MUFU reciprocal square root.
  * count must be >= 6.  The roofline model of the field kernels charges each
  * divide, square root and logarithm rates[0] / rates[k] FP64-pipe slots. */
 int ccoil_measure_op_rates(double *rates, int count);
+
+/* Diagnostic with no counterpart in the reference: evaluates the natural
+ * logarithm that the FP64 vector-potential integrand uses (Cody-Waite range
+ * reduction and the atanh series, within about 1 ulp) at n points, for checks
+ * against other implementations.  x and out are device pointers of n doubles;
+ * every x must be positive, normal and finite.  Synchronous on `stream`. */
+int ccoil_eval_log64(const double *x, double *out, long long n, void *stream);
 
 #ifdef __cplusplus
 }
