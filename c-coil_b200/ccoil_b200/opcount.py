@@ -35,9 +35,9 @@ OPS_PER_NODE_64 = {
 # the kernel evaluates mirror pairs of nodes, so these are half the count of
 # one pair step (both nodes' integrands and the pair's accumulation)
 OPS_PER_NODE_32 = {
-    (0, True): (27, 3), (0, False): (4, 1),
+    (0, True): (24.5, 3), (0, False): (4, 1),
     (1, True): (26, 3), (1, False): (10.5, 1),
-    (3, True): (39.5, 5), (3, False): (16.5, 1),
+    (3, True): (39.5, 5), (3, False): (13.5, 1),
 }
 # algorithmic flops per node: every operation of the reference integrand counts one
 FLOPS_PER_NODE = {k: sum(v) for k, v in OPS_PER_NODE_64.items()}
