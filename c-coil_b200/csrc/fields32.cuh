@@ -54,7 +54,7 @@ struct NearPair
 
 // CTAs per SM the register allocation targets, measured best on B200 over
 // 4-8 (2^20 points, 128-coil group): 6 for the vector potential, 5 for B,
-// 4 for the gradient (126 registers, no spills: 3.5 % faster than 5 CTAs
+// 4 for the gradient (124 registers, no spills: 3.5 % faster than 5 CTAs
 // with 96 registers and spills; 3 CTAs was no faster)
 #ifndef CCOIL_FP32_MIN_BLOCKS_A
 #define CCOIL_FP32_MIN_BLOCKS_A 6
