@@ -89,9 +89,27 @@ struct SegmentSet
     int max_bytes = 0;
 };
 
+// Destination of the segment builder: the blob bytes, appended in order (every
+// entry keeps 16-byte alignment), and one descriptor per finished segment.  A
+// sink with fixed capacity returns false when full; overflowMessage() then
+// names the limit that was reached.
+struct SegmentSink
+{
+    virtual bool append(const void *p, size_t n) = 0;
+    virtual size_t size() const = 0;
+    virtual bool segment(const SegmentDesc &d) = 0;
+    virtual std::string overflowMessage() const = 0;
+
+  protected:
+    ~SegmentSink() = default;
+};
+
 // Builds the segment list for `coils` (each at its own precision) for field
 // evaluation; precision selects whether FP32 tables are appended.
 bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err);
+// The same layout written into any sink (the allocation-free entry point's
+// fixed staging buffers use this form).
+bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSink &out, std::string &err);
 // FP32 angular pair table of a coil at precision p: (n + 1) / 2 entries, entry i
 // for nodes i and n-1-i of the FP64 table in its reference order
 void buildPhiPairs32(const PrecisionArgs &p, std::vector<PhiNode32> &out);

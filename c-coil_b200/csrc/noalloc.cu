@@ -31,9 +31,6 @@ constexpr size_t kOffWork = kOffSegs + sizeof(SegmentDesc) * kStaticMaxSegments;
 constexpr size_t kOffCount = kOffWork + kNearPairBytes * kStaticWorkEntries;
 constexpr size_t kStaticScratchBytes = kOffCount + 256;
 constexpr int kMaxDevices = 64;
-constexpr double kPi = 3.14159265358979323846;
-constexpr double kMuReduced = 1e-7;
-constexpr double kNearMarginStatic = 0.1;  // same near-field box as the plan path's default
 
 // The scratch.  In host code this name is only a stand-in: its device address
 // comes from cudaGetSymbolAddress, once per device.
@@ -47,134 +44,58 @@ std::mutex g_hostMutex;
 unsigned char *g_deviceScratch[kMaxDevices] = {};
 std::mutex g_setupMutex;
 
-struct Writer
+// The fixed host staging buffers as a segment sink: the node-table layout is
+// the plan path's own (buildFieldSegments), only its destination differs.
+struct StaticSink final : SegmentSink
 {
-    unsigned char *base;
-    size_t cap, used = 0;
-    bool ok = true;
-    void put(const void *p, size_t n)
+    size_t used = 0;
+    int nseg = 0;
+    bool tablesFull = false, segmentsFull = false;
+    bool append(const void *p, size_t n) override
     {
-        if (!ok || used + n > cap)
+        if (used + n > kStaticBlobBytes)
         {
-            ok = false;
-            return;
+            tablesFull = true;
+            return false;
         }
-        std::memcpy(base + used, p, n);
+        std::memcpy(g_hostBlob + used, p, n);
         used += n;
+        return true;
+    }
+    size_t size() const override { return used; }
+    bool segment(const SegmentDesc &d) override
+    {
+        if (nseg >= kStaticMaxSegments)
+        {
+            segmentsFull = true;
+            return false;
+        }
+        g_hostSegs[nseg++] = d;
+        return true;
+    }
+    std::string overflowMessage() const override
+    {
+        return segmentsFull ? "coil set needs more than 8192 segments; the static entry point's limit"
+                            : "coil set needs more than 1 MiB of node tables; the static entry point's limit";
     }
 };
 
-// Builds the same segment layout as buildFieldSegments (segments.cpp) for the
-// FP32-compensated path, computing every node on the fly instead of holding
-// per-coil tables.
+// Builds the FP32-compensated segment layout of `coils` into the staging buffers.
 int buildStatic(const Coil *coils, int count, int field, size_t &blobBytes, int &nseg)
 {
-    Writer w{g_hostBlob, kStaticBlobBytes};
-    nseg = 0;
-    for (int ci = 0; ci < count; ++ci)
-    {
-        const Coil &k = coils[ci];
-        const PrecisionArgs &p = k.precision;
-        if (!validArgs(p))
-            return failMessage(CCOIL_ERR_INVALID_ARGUMENT,
-                               "a coil's precision arguments are out of range (increments 1..100, blocks >= 1)");
-        if (!(k.inner_radius > 0.0) || !(k.thickness > 0.0) || !(k.length > 0.0))
-            return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "inner radius, thickness and length must be positive");
-        const bool fast = k.use_fast_method != 0;
-        const double tBlock = k.thickness / p.thickness_blocks, aBlock = kPi / p.angular_blocks;
-        const double constant = fast ? kMuReduced * k.current_density * tBlock * aBlock * 2 * 0.25
-                                     : kMuReduced * k.current_density * (k.length / p.length_blocks) * tBlock *
-                                           aBlock * 2 * 0.125;
-        const int nt = p.thickness_blocks * p.thickness_increments;
-        const int nl = fast ? 0 : p.length_blocks * p.length_increments;
-        const int nphi = p.angular_blocks * p.angular_increments;
-        const int headerBytes = (int)sizeof(SegmentHeader);
-        const int fixedBytes = headerBytes + 16 * (nt + nl);
-        // 16 bytes per FP64 node plus 16 per FP32 mirror-pair entry; segments cut
-        // at even node counts so that no mirror pair is split
-        const int maxPhi = 2 * ((kSegmentBytes - fixedBytes) / 48);
-        if (maxPhi < 1)
-            return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "a coil's thickness/length node tables exceed one segment");
-        const double *tx = legendreNodes(p.thickness_increments), *tw = legendreWeights(p.thickness_increments);
-        const double *ax = legendreNodes(p.angular_increments), *aw = legendreWeights(p.angular_increments);
-        auto phiOf = [&](int j) {
-            return aBlock * (j / p.angular_increments + 0.5) + (aBlock * 0.5) * ax[j % p.angular_increments];
-        };
-        for (int start = 0; start < nphi; start += maxPhi)
-        {
-            const int cnt = nphi - start < maxPhi ? nphi - start : maxPhi;
-            if (nseg >= kStaticMaxSegments)
-                return failMessage(CCOIL_ERR_INVALID_ARGUMENT,
-                                   "coil set needs more than 8192 segments; the static entry point's limit");
-            SegmentHeader h;
-            std::memset(&h, 0, sizeof(h));
-            std::memcpy(h.position, k.position, sizeof(h.position));
-            std::memcpy(h.inv_transform, k.inverse_transform, sizeof(h.inv_transform));
-            std::memcpy(h.transform, k.transform, sizeof(h.transform));
-            h.half_length = k.length * 0.5;
-            h.field_factor = field == CCOIL_FIELD_E ? 2 * kPi * k.sine_frequency : 1.0;
-            h.inner_radius = k.inner_radius;
-            h.n_t = nt;
-            h.n_l = nl;
-            h.n_phi = cnt;
-            h.fast = fast ? 1 : 0;
-            h.off_t = headerBytes / 16;
-            h.off_l = h.off_t + nt;
-            h.off_phi = h.off_l + nl;
-            h.off_f32 = h.off_phi + cnt;
-            const double margin = kNearMarginStatic * k.inner_radius;
-            h.near_lo[0] = k.inner_radius - margin;
-            h.near_hi[0] = k.inner_radius + k.thickness + margin;
-            h.near_lo[1] = -0.5 * k.length - margin;
-            h.near_hi[1] = 0.5 * k.length + margin;
-            h.near_r2 = margin * margin;
-
-            SegmentDesc &d = g_hostSegs[nseg];
-            d.offset = (long long)w.used;
-            d.coil = ci;
-            w.put(&h, sizeof(h));
-            for (int bt = 0; bt < p.thickness_blocks; ++bt)
-                for (int i = 0; i < p.thickness_increments; ++i)
-                {
-                    double e[2] = {k.inner_radius + tBlock * (bt + 0.5) + (tBlock * 0.5) * tx[i], constant * tw[i]};
-                    w.put(e, sizeof(e));
-                }
-            if (!fast)
-            {
-                const double lBlock = k.length / p.length_blocks;
-                const double *lx = legendreNodes(p.length_increments), *lw = legendreWeights(p.length_increments);
-                for (int bl = 0; bl < p.length_blocks; ++bl)
-                    for (int i = 0; i < p.length_increments; ++i)
-                    {
-                        double e[2] = {-k.length * 0.5 + lBlock * (bl + 0.5) + (lBlock * 0.5) * lx[i], lw[i]};
-                        w.put(e, sizeof(e));
-                    }
-            }
-            // the FP64 table in mirror-pair order, then the pair entries it covers
-            for (int j = start; j < start + cnt; ++j)
-            {
-                const int node = pairOrderNode(j, nphi);
-                double e[2] = {std::cos(phiOf(node)), aw[node % p.angular_increments]};
-                w.put(e, sizeof(e));
-            }
-            for (int i = start / 2; i < (start + cnt + 1) / 2; ++i)
-            {
-                const PhiNode32 nd = phiPair32(p, i);
-                w.put(&nd, sizeof(nd));
-            }
-            d.bytes = (int)(w.used - (size_t)d.offset);
-            if (!w.ok)
-                return failMessage(CCOIL_ERR_INVALID_ARGUMENT,
-                                   "coil set needs more than 1 MiB of node tables; the static entry point's limit");
-            ++nseg;
-        }
-    }
-    blobBytes = w.used;
+    StaticSink sink;
+    std::string err;
+    if (!buildFieldSegments(coils, count, field, CCOIL_PRECISION_FP32_COMPENSATED, sink, err))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, err);
+    blobBytes = sink.used;
+    nseg = sink.nseg;
     return CCOIL_OK;
 }
 
 // Device address of the scratch array on the current device, looked up once per
-// device with that device current.
+// device with that device current.  The address stays cached for the life of
+// the process: cudaDeviceReset, which unloads the module, is not supported while
+// the library is in use.
 int scratchAddress(unsigned char **out)
 {
     int dev = 0;

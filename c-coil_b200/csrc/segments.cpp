@@ -100,11 +100,8 @@ void setNearBox(const Coil &k, SegmentHeader &h)
     h.near_r2 = margin * margin;
 }
 
-bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err)
+bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSink &out, std::string &err)
 {
-    out.blob.clear();
-    out.segs.clear();
-    out.max_bytes = 0;
     const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
 
     for (int ci = 0; ci < count; ++ci)
@@ -208,19 +205,53 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
             setNearBox(k, h);
 
             SegmentDesc d;
-            d.offset = (long long)out.blob.size();
+            d.offset = (long long)out.size();
             d.coil = ci;
-            appendBytes(out.blob, &h, sizeof(h));
-            appendBytes(out.blob, tNodes.data(), 16 * tNodes.size());
-            appendBytes(out.blob, lNodes.data(), 16 * lNodes.size());
-            appendBytes(out.blob, phiNodes.data() + start, 16 * (size_t)cnt);
-            if (fp32)
-                appendBytes(out.blob, phi32.data() + start / 2, 16 * (size_t)((cnt + 1) / 2));
-            d.bytes = (int)(out.blob.size() - d.offset);
-            out.max_bytes = std::max(out.max_bytes, d.bytes);
-            out.segs.push_back(d);
+            bool ok = out.append(&h, sizeof(h)) && out.append(tNodes.data(), 16 * tNodes.size()) &&
+                      out.append(lNodes.data(), 16 * lNodes.size()) &&
+                      out.append(phiNodes.data() + start, 16 * (size_t)cnt);
+            if (ok && fp32)
+                ok = out.append(phi32.data() + start / 2, 16 * (size_t)((cnt + 1) / 2));
+            d.bytes = (int)((long long)out.size() - d.offset);
+            if (!ok || !out.segment(d))
+            {
+                err = out.overflowMessage();
+                return false;
+            }
         }
     }
     return true;
+}
+
+namespace
+{
+// The plan path's sink: growable host vectors.
+struct VectorSink final : SegmentSink
+{
+    SegmentSet &set;
+    explicit VectorSink(SegmentSet &s) : set(s) {}
+    bool append(const void *p, size_t n) override
+    {
+        appendBytes(set.blob, p, n);
+        return true;
+    }
+    size_t size() const override { return set.blob.size(); }
+    bool segment(const SegmentDesc &d) override
+    {
+        set.max_bytes = std::max(set.max_bytes, d.bytes);
+        set.segs.push_back(d);
+        return true;
+    }
+    std::string overflowMessage() const override { return "segment tables could not be stored"; }
+};
+} // namespace
+
+bool buildFieldSegments(const Coil *coils, int count, int field, int precision, SegmentSet &out, std::string &err)
+{
+    out.blob.clear();
+    out.segs.clear();
+    out.max_bytes = 0;
+    VectorSink sink(out);
+    return buildFieldSegments(coils, count, field, precision, sink, err);
 }
 } // namespace ccoil

@@ -321,8 +321,10 @@ long long ccoil_timeout_count(void);
  * PrecisionFactor 5), 8192 segments and 2^31-1 points; larger requests return
  * CCOIL_ERR_INVALID_ARGUMENT with a message.  The first call on a device looks
  * up the array's device address; make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
- * streams or host threads) race and must be ordered by the caller. */
+ * capture.  The address is kept for the life of the process, so
+ * cudaDeviceReset is not supported while the library is in use.  All calls
+ * share the array: calls that overlap on the GPU (other streams or host
+ * threads) race and must be ordered by the caller. */
 int ccoil_fields_fp32c_static(const ccoil_coil_t *coils, int coil_count, const double *points,
                               long long point_count, int field, double *out, void *stream);
 

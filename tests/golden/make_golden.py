@@ -42,7 +42,9 @@ sys.path.insert(0, os.path.join(ROOT, "c-coil_b200"))
 from oracle import Reference, coil_row  # noqa: E402
 from ccoil_b200 import workloads  # noqa: E402
 
-REF_DATA = "/root/reference/data/values_MInductance_general.txt"
+# the reference checkout: CCOIL_REFERENCE (default: where the build container mounts it)
+REF_ROOT = os.environ.get("CCOIL_REFERENCE", "/root/reference")
+REF_DATA = os.path.join(REF_ROOT, "data", "values_MInductance_general.txt")
 
 
 def main():

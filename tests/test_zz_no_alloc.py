@@ -31,7 +31,9 @@ def test_static_entry_point_matches_plan_path(ccoil):
                           workloads.points_cube(2000, seed=316, half=0.5) + 0.5])
     dpts = torch.from_numpy(pts).cuda()
     stream = torch.cuda.current_stream().cuda_stream
-    for field in (1, 3, 0):
+    # B, G, A and E (E = 2 pi f A: the rows carry f = 50 Hz); the rows mix all four
+    # coil types, so both the fast (RECTANGULAR, THIN) and slow integrands run
+    for field in (1, 3, 0, 2):
         width = 9 if field == 3 else 3
         plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_COMPENSATED)
         expected = plan(pts)
