@@ -179,6 +179,22 @@ struct BatchLaunch
     unsigned long long *d_work_count = nullptr;
 };
 constexpr size_t kBatchItemBytes = 32;
+
+// pairs.cu: the arrangement evaluator behind ccoil_pair_arrangements_zaxis,
+// with two options its C-ABI callers leave at their defaults: full_ring makes
+// every arrangement integrate the whole secondary ring (the reference's GPU
+// kernels never take the CPU path's half-ring rule for coplanar axes), and
+// scale multiplies the result.
+struct PairOptions
+{
+    bool full_ring = false;
+    double scale = 1.0;
+};
+int pairArrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                     const ccoil_precision_args_t *secondary_precisions, const ccoil_precision_args_t *zaxis_precisions,
+                     const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses, long long count,
+                     int quantity, int precision, double *out, long long *z_axis_count, int memory, void *stream,
+                     const PairOptions &opt);
 int launchBatch(const BatchLaunch &B, void *stream);
 int batchBlocksPerSM(int precision);
 } // namespace ccoil

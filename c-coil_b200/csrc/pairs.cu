@@ -47,7 +47,9 @@ struct alignas(16) PairHeader
     double prim_y_angle; // the primary's own orientation (used when primaries do not move)
     double prim_z_angle;
     int s_nl, s_nt, s_na, s_ablocks;  // secondary node counts and angular blocks
-    int off_sl, off_st, off_sa, pad2; // secondary tables (16-byte units from the header)
+    int off_sl, off_st, off_sa;       // secondary tables (16-byte units from the header)
+    int full_ring;                    // 1: always integrate the whole secondary ring (the reference's GPU
+                                      // kernels), 0: half ring for coplanar axes (its CPU path)
     // parameter-gradient tables (16-byte units; 0 when absent): d(node position)/d(dimension)
     // of the primary's thickness and length nodes and of the secondary's length and
     // thickness nodes, i.e. the nodes' positions on [0, 1] (thickness) or [-1/2, 1/2] (length)
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                 S.skip = skip ? 1 : 0;
                 hasZ = hasZ || skip;
                 double offset = 0.0;
-                const bool improved = QTY != 1 ? improvedCase(ppose, spose, offset) : false;
+                const bool improved = QTY != 1 && !ph.full_ring ? improvedCase(ppose, spose, offset) : false;
                 for (int i = 0; i < 3; ++i)
                 {
                     S.pos[i] = P.pos[i];
@@ -755,7 +757,7 @@ void primaryTables(const Coil &prim, const PrecisionArgs &pp, std::vector<double
 // (CalculateFieldsFast.cxx:17-55, CalculateFieldsSlow.cxx:17-66), secondary
 // cloud as CalculateMInductanceGeneral.cxx:41-103 builds it.
 bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const PrecisionArgs &spa, bool fp32,
-               bool units, std::vector<unsigned char> &blob, std::string &err)
+               bool units, const PairOptions &opt, std::vector<unsigned char> &blob, std::string &err)
 {
     if (!validArgs(pp) || !validArgs(spa))
     {
@@ -857,8 +859,9 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
         ph.off_stu = ph.off_slu + (int)slu_.size() / 2;
     }
     const double blocks = double(spa.length_blocks) * spa.thickness_blocks * spa.angular_blocks;
-    ph.m_factor = 2 * kPi * sec.num_turns / prim.current / blocks;
-    ph.f_factor = 2 * kPi * (sec.current * sec.num_turns) / blocks;
+    ph.m_factor = 2 * kPi * sec.num_turns / prim.current / blocks * opt.scale;
+    ph.f_factor = 2 * kPi * (sec.current * sec.num_turns) / blocks * opt.scale;
+    ph.full_ring = opt.full_ring ? 1 : 0;
     ph.prim_y_angle = prim.y_axis_angle;
     ph.prim_z_angle = prim.z_axis_angle;
     put(blob, &ph, sizeof(ph));
@@ -903,13 +906,11 @@ int cudaFail(cudaError_t e, const char *what);
 
 using namespace ccoil;
 
-extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int primary_count,
-                                             const ccoil_coil_t *secondary,
-                                             const ccoil_precision_args_t *secondary_precisions,
-                                             const ccoil_precision_args_t *zaxis_precisions,
-                                             const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
-                                             long long count, int quantity, int precision, double *out,
-                                             long long *z_axis_count, int memory, void *stream)
+int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
+                            const ccoil_precision_args_t *secondary_precisions,
+                            const ccoil_precision_args_t *zaxis_precisions, const ccoil_pose_t *primary_poses,
+                            const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
+                            double *out, long long *z_axis_count, int memory, void *stream, const PairOptions &opt)
 {
     if (primary_count < 0 || (primary_count > 0 && (!primaries || !secondary_precisions)) || !secondary)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "null coils or negative primary_count");
@@ -955,7 +956,7 @@ extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int 
     {
         offsets.push_back((long long)blob.size());
         if (!buildPair(primaries[j], *secondary, primaries[j].precision, secondary_precisions[j], fp32,
-                       quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, blob, err))
+                       quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, opt, blob, err))
             return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
     }
     const size_t generalBytes = blob.size();
@@ -1074,6 +1075,19 @@ extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int 
     if (z_axis_count)
         *z_axis_count = (long long)zcount;
     return CCOIL_OK;
+}
+
+extern "C" int ccoil_pair_arrangements_zaxis(const ccoil_coil_t *primaries, int primary_count,
+                                             const ccoil_coil_t *secondary,
+                                             const ccoil_precision_args_t *secondary_precisions,
+                                             const ccoil_precision_args_t *zaxis_precisions,
+                                             const ccoil_pose_t *primary_poses, const ccoil_pose_t *secondary_poses,
+                                             long long count, int quantity, int precision, double *out,
+                                             long long *z_axis_count, int memory, void *stream)
+{
+    return pairArrangements(primaries, primary_count, secondary, secondary_precisions, zaxis_precisions,
+                            primary_poses, secondary_poses, count, quantity, precision, out, z_axis_count, memory,
+                            stream, PairOptions{});
 }
 
 extern "C" int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,

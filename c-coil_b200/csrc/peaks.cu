@@ -55,6 +55,26 @@ __global__ void fma32Kernel(float *sink, int iters, float a, float b)
         sink[0] = s;
 }
 
+// packed FP32 (sm_100 fma.rn.f32x2): one instruction, two FMAs
+__global__ void fma32x2Kernel(float *sink, int iters, float a, float b)
+{
+    float2 v[kChains];
+#pragma unroll
+    for (int i = 0; i < kChains; ++i)
+        v[i] = make_float2(threadIdx.x * 1e-3f + i, threadIdx.x * 2e-3f + i);
+    const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int i = 0; i < kChains; ++i)
+            v[i] = __ffma2_rn(v[i], a2, b2);
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kChains; ++i)
+        s += v[i].x + v[i].y;
+    if (s == 1.2345f)
+        sink[0] = s;
+}
+
 __global__ void mufuKernel(float *sink, int iters)
 {
     float v[kChains];
@@ -138,7 +158,7 @@ using namespace ccoil;
 extern "C" int ccoil_measure_op_rates(double *rates, int count)
 {
     if (!rates || count < 6)
-        return fail(CCOIL_ERR_INVALID_ARGUMENT, "rates needs 6 entries");
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "rates needs at least 6 entries");
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess)
@@ -158,6 +178,8 @@ extern "C" int ccoil_measure_op_rates(double *rates, int count)
     float msDiv = timeIt([&] { op64Kernel<0><<<blocks, threads>>>((double *)sink, itOp); });
     float msSqrt = timeIt([&] { op64Kernel<1><<<blocks, threads>>>((double *)sink, itOp); });
     float msLog = timeIt([&] { op64Kernel<2><<<blocks, threads>>>((double *)sink, itOp); });
+    float ms32x2 = count > 6 ? timeIt([&] { fma32x2Kernel<<<blocks, threads>>>((float *)sink, it32, 0.999999f, 1e-7f); })
+                             : 0.0f;
     e = cudaGetLastError();
     cudaFree(sink);
     if (e != cudaSuccess)
@@ -175,6 +197,8 @@ extern "C" int ccoil_measure_op_rates(double *rates, int count)
     rates[3] = rate(msLog);
     rates[4] = lanes * it32 / (ms32 * 1e-3);             // FP32 FMA instructions per second
     rates[5] = lanes * itMufu / (msMu * 1e-3);           // MUFU rsqrt per second
+    if (count > 6)
+        rates[6] = lanes * it32 / (ms32x2 * 1e-3);       // packed FP32 FMA instructions (2 FMAs each) per second
     return CCOIL_OK;
 }
 

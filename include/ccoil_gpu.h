@@ -338,8 +338,9 @@ int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops, double *m
  * per second, whole device) of rates[0] FP64-pipe instructions (FMA),
  * rates[1] __ddiv_rn, rates[2] __dsqrt_rn, rates[3] the FP64 integrands'
  * logarithm (see ccoil_eval_log64),
- * rates[4] FP32 FMA instructions, rates[5] MUFU reciprocal square root.
- * count must be >= 6.  The roofline model of the field kernels charges each
+ * rates[4] FP32 FMA instructions, rates[5] MUFU reciprocal square root and,
+ * when count >= 7, rates[6] packed FP32 FMA instructions (fma.rn.f32x2, two
+ * FMAs each).  count must be >= 6.  The roofline model of the field kernels charges each
  * divide, square root and logarithm rates[0] / rates[k] FP64-pipe slots. */
 int ccoil_measure_op_rates(double *rates, int count);
 

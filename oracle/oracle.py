@@ -17,6 +17,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libccoil_ref.so")
+# the same reference sources built with USE_GPU: its own GPU glue, linked against
+# libccoil_b200.so (oracle/Makefile, target ref-gpu)
+REF_GPU_SO = os.path.join(HERE, "_ref", "libccoil_ref_gpu.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -135,6 +138,8 @@ class Reference:
         L.ref_pair_args.argtypes = [_dp, _dp, _d, _i, _i, _i, _ip]
         L.ref_coil_fields.argtypes = [_dp, _d, _ip, _i, _i, _ll, _dp, _dp]
         L.ref_group_fields.argtypes = [_i, _dp, _d, _i, _i, _ll, _dp, _dp]
+        if hasattr(L, "ref_group_fields_dispatch"):
+            L.ref_group_fields_dispatch.argtypes = [_i, _dp, _d, _i, _i, _ll, _dp, _dp]
         L.ref_mutual_inductance.argtypes = [_dp, _dp, _d, _i, _dp]
         L.ref_mutual_inductance_args.argtypes = [_dp, _dp, _ip, _i, _dp]
         L.ref_force_torque.argtypes = [_dp, _dp, _d, _i, _dp]
@@ -175,6 +180,12 @@ class Reference:
         self._check(self.lib.ref_precision_args(_ptr(_f64(coil)), pf, int(gpu), _ptr(out, _ip)))
         return out
 
+    def secondary_precision_gpu(self, coil, pf):
+        """PrecisionArguments::getSecondaryCoilPrecisionArgumentsGPU"""
+        out = np.zeros(6, dtype=np.int32)
+        self._check(self.lib.ref_secondary_precision_gpu(_ptr(_f64(coil)), pf, _ptr(out, _ip)))
+        return out
+
     def pair_args(self, prim, sec, pf, gpu=False, z_axis=False, pure_gpu=False):
         out = np.zeros(12, dtype=np.int32)
         self._check(self.lib.ref_pair_args(_ptr(_f64(prim)), _ptr(_f64(sec)), pf, int(gpu), int(z_axis),
@@ -197,6 +208,17 @@ class Reference:
         out = np.zeros((n, 9 if qty == 3 else 3))
         self._check(self.lib.ref_group_fields(coils.shape[0], _ptr(coils), pf, qty, method, n, _ptr(pts),
                                               _ptr(out)))
+        return out
+
+    def group_fields_dispatch(self, coils, points, qty, pf=5.0, method=0):
+        """CoilGroup::computeAll*(points, method) through the group's own dispatch
+        (method 2: its GPU glue)."""
+        pts = _f64(points)
+        coils = _f64(coils)
+        n = pts.shape[0]
+        out = np.zeros((n, 9 if qty == 3 else 3))
+        self._check(self.lib.ref_group_fields_dispatch(coils.shape[0], _ptr(coils), pf, qty, method, n, _ptr(pts),
+                                                       _ptr(out)))
         return out
 
     def mutual_inductance(self, prim, sec, pf=5.0, args=None, method=0):

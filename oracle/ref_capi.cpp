@@ -83,7 +83,9 @@ void fromArgs(const PrecisionArguments &a, int *out)
     out[5] = a.lengthIncrements;
 }
 
-ComputeMethod toMethod(int m) { return m == 1 ? CPU_MT : CPU_ST; }
+// 0 = CPU_ST, 1 = CPU_MT, 2 = GPU (a build with USE_GPU, linked against
+// libccoil_b200.so, whose exports stand in for the reference's CUDA kernels)
+ComputeMethod toMethod(int m) { return m == 2 ? GPU : (m == 1 ? CPU_MT : CPU_ST); }
 
 void coilFields(const Coil &coil, const PrecisionArguments &prec, int qty, ComputeMethod method,
                 const vec3::Vector3Array &pts, double *out, bool accumulate)
@@ -180,7 +182,8 @@ int ref_pair_args(const double *p, const double *s, double pf, int gpu, int zAxi
 }
 
 // One coil: fields at n points with explicit precision args (prec6) or, if prec6
-// is null, the coil's default CPU precision at pf.  method 0 = CPU_ST, 1 = CPU_MT.
+// is null, the coil's default CPU precision at pf.  method 0 = CPU_ST, 1 = CPU_MT,
+// 2 = GPU.
 int ref_coil_fields(const double *c, double pf, const int *prec6, int qty, int method, long long n,
                     const double *pts, double *out)
 {
@@ -210,6 +213,31 @@ int ref_group_fields(int ncoils, const double *coils, double pf, int qty, int me
         {
             auto coil = makeCoil(coils + 11 * k, pf);
             coilFields(*coil, coil->getPrecisionSettingsCPU(), qty, toMethod(method), arr, out, true);
+        }
+        return 0;
+    } catch (...) { return -1; }
+}
+
+// A group through the reference's own group dispatch, CoilGroup::computeAll*(points, method)
+// (src/CoilGroup/Fields/ComputeFields.cxx): with method 2 (GPU) its glue packs every member
+// at its GPU precision for pf (src/CoilGroup/Utils/GPUArgumentGeneration.cxx:17-95) and calls
+// Calculate_hardware_accelerated_*_group.
+int ref_group_fields_dispatch(int ncoils, const double *coils, double pf, int qty, int method, long long n,
+                              const double *pts, double *out)
+{
+    try
+    {
+        std::vector<std::shared_ptr<Coil>> members;
+        for (int k = 0; k < ncoils; ++k)
+            members.push_back(makeSharedCoil(coils + 11 * k, pf));
+        CoilGroup group(members, PrecisionFactor(pf), g_threads);
+        vec3::Vector3Array arr = toArray(n, pts);
+        switch (qty)
+        {
+            case QTY_A: putVectors(group.computeAllAPotentialVectors(arr, toMethod(method)), out); break;
+            case QTY_B: putVectors(group.computeAllBFieldVectors(arr, toMethod(method)), out); break;
+            case QTY_E: putVectors(group.computeAllEFieldVectors(arr, toMethod(method)), out); break;
+            default: putMatrices(group.computeAllBGradientMatrices(arr, toMethod(method)), out); break;
         }
         return 0;
     } catch (...) { return -1; }

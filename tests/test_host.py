@@ -16,6 +16,41 @@ def test_library_exports_every_header_symbol(ccoil):
     assert not missing, missing
 
 
+# The reference's GPU entry points (include/ccoil_reference_abi.h) with their C++
+# names, as g++ mangles them for the TYPE=double structs
+REFERENCE_ENTRY_SYMBOLS = [
+    "_Z32Calculate_hardware_accelerated_ax8CoilDataPK10VectorDataPS0_",
+    "_Z32Calculate_hardware_accelerated_bx8CoilDataPK10VectorDataPS0_",
+    "_Z32Calculate_hardware_accelerated_gx8CoilDataPK10VectorDataP10MatrixData",
+    "_Z42Calculate_mutual_inductance_configurationsxxPK21CoilPairArgumentsDataPK20CoilPairPositionDataPd",
+    "_Z41Calculate_force_and_torque_configurationsxxPK21CoilPairArgumentsDataPK20CoilPairPositionDataP15ForceTorqueData",
+    "_Z38Calculate_hardware_accelerated_a_groupxxPK8CoilDataPK10VectorDataPS2_",
+    "_Z38Calculate_hardware_accelerated_b_groupxxPK8CoilDataPK10VectorDataPS2_",
+    "_Z38Calculate_hardware_accelerated_e_groupxxPK8CoilDataPK10VectorDataPS2_",
+    "_Z38Calculate_hardware_accelerated_g_groupxxPK8CoilDataPK10VectorDataP10MatrixData",
+    "_Z48Calculate_mutual_inductance_configurations_groupxxx17SecondaryCoilDataPK8CoilDataPK25SecondaryCoilPositionDataPd",
+    "_Z47Calculate_force_and_torque_configurations_groupxxx17SecondaryCoilDataPK8CoilDataPK25SecondaryCoilPositionDataP15ForceTorqueData",
+]
+
+
+def test_library_exports_the_reference_entry_points(ccoil):
+    lib = ccoil.lib()
+    missing = [n for n in REFERENCE_ENTRY_SYMBOLS if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_reference_gpu_glue_links_against_the_library(ccoil):
+    """The reference's unmodified GPU glue (built with USE_GPU, oracle/Makefile target
+    ref-gpu, linked with --no-undefined) loads with this library standing in for its
+    CUDA kernels."""
+    from oracle import Reference, REF_GPU_SO
+    if not Reference.available(REF_GPU_SO):
+        pytest.skip("oracle/_ref/libccoil_ref_gpu.so not built (needs the reference sources)")
+    ccoil.lib()
+    glue = Reference(REF_GPU_SO)
+    assert hasattr(glue.lib, "ref_group_fields_dispatch")
+
+
 def test_abi_version(ccoil):
     assert ccoil.lib().ccoil_abi_version() == 1
 

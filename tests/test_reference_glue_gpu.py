@@ -1,0 +1,132 @@
+"""The reference's own GPU host glue, compiled unmodified with USE_GPU and linked
+against libccoil_b200.so (oracle/Makefile, target ref-gpu).
+
+Coil::computeAll*(points, GPU), CoilGroup::computeAll*(points, GPU) and the
+arrangement functions with ComputeMethod::GPU run the reference's packing code
+(Coil::generateCoilData, CoilGroup::generateCoilDataArray,
+Coil::generateCoilPairArgumentsData, CoilGroup::generateSecondaryData) and reach
+this library through the Calculate_* entry points declared in
+include/ccoil_reference_abi.h, which stand in for the reference's CUDA kernels.
+
+Each result is compared with the reference's own CPU path at the precision
+arguments the glue used (the GPU ones, capped at GPU_INCREMENTS = 80): 1e-12,
+the FP64 kernels' parity bar.  The glue's own quirks come through as they are:
+the coil-level force glue passes the correction factor 2 pi N2 / I1, so its
+force is the CPU force divided by I1 I2, and the group arrangement glue halves
+the PrecisionFactor."""
+import numpy as np
+import pytest
+
+from conftest import gradient_band, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+GPU = 2  # ComputeMethod::GPU in the reference's C-API wrapper
+
+
+@pytest.fixture(scope="module")
+def glue():
+    import ccoil_b200
+    ccoil_b200.lib()
+    from oracle import Reference, REF_GPU_SO
+    if not Reference.available(REF_GPU_SO):
+        pytest.skip("oracle/_ref/libccoil_ref_gpu.so not built (needs the reference sources)")
+    return Reference(REF_GPU_SO)
+
+
+# {R, a, b, N, I, f, x, y, z, yAngle, zAngle}: RECTANGULAR, THIN, FLAT, FILAMENT
+ROWS = np.array([[0.1, 0.05, 0.08, 120, 1.5, 60.0, 0.05, -0.02, 0.1, 0.7, 0.3],
+                 [0.12, 0.0, 0.1, 90, -2.0, 50.0, 0.0, 0.03, 0.0, 0.2, 1.1],
+                 [0.08, 0.04, 0.0, 150, 0.7, 40.0, -0.02, 0.0, 0.05, 2.0, 0.0],
+                 [0.1, 0.0, 0.0, 60, 3.0, 30.0, -0.1, 0.0, 0.05, 0.4, 2.5]])
+
+
+def points(n, seed, half=0.5):
+    return np.random.default_rng(seed).uniform(-half, half, (n, 3))
+
+
+def check(got, exp, rows, pts, qty):
+    e = rel_err(got, exp)
+    if qty == 3:
+        band = gradient_band(rows, pts)
+        assert e[band].max(initial=0.0) < 1e-5
+        e = e[~band]
+    assert e.max() < TOL, (qty, e.max())
+
+
+@pytest.mark.parametrize("qty", [0, 1, 2, 3])
+def test_coil_fields(glue, qty):
+    pts = points(2048, 11)
+    for row in ROWS:
+        prec = glue.precision_args(row, 5.0, gpu=True)
+        got = glue.coil_fields(row, pts, qty, pf=5.0, prec=prec, method=GPU)
+        exp = glue.coil_fields(row, pts, qty, pf=5.0, prec=prec, method=0)
+        check(got, exp, row[None, :], pts, qty)
+
+
+@pytest.mark.parametrize("qty", [0, 1, 2, 3])
+def test_group_fields(glue, qty):
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(12, seed=31)
+    pts = points(2048, 12, half=1.0)
+    got = glue.group_fields_dispatch(rows, pts, qty, pf=5.0, method=GPU)
+    exp = np.zeros_like(got)
+    for row in rows:
+        exp += glue.coil_fields(row, pts, qty, pf=5.0, prec=glue.precision_args(row, 5.0, gpu=True), method=0)
+    check(got, exp, rows, pts, qty)
+
+
+def arrangements(n, seed):
+    g = np.random.default_rng(seed)
+    return (g.uniform(-0.05, 0.05, (n, 3)), g.uniform(-0.3, 0.3, (n, 3)), g.uniform(0, np.pi, n),
+            g.uniform(0, 2 * np.pi, n), g.uniform(0, np.pi, n), g.uniform(0, 2 * np.pi, n))
+
+
+def posed(row, pos, y, z):
+    r = row.copy()
+    r[6:9] = pos
+    r[9], r[10] = y, z
+    return r
+
+
+def test_coil_arrangements(glue):
+    prim = np.array([0.1, 0.05, 0.1, 200, 2.0, 50.0, 0, 0, 0, 0, 0])
+    sec = np.array([0.05, 0.0, 0.2, 100, 3.0, 50.0, 0, 0, 0, 0, 0])
+    n = 48
+    pp, sp, py, pz, sy, sz = arrangements(n, 21)
+    m = glue.m_arrangements(prim, sec, pp, sp, py, pz, sy, sz, pf=5.0, method=GPU)
+    ft = glue.ft_arrangements(prim, sec, pp, sp, py, pz, sy, sz, pf=5.0, method=GPU)
+    args = glue.pair_args(prim, sec, 5.0, gpu=True, pure_gpu=True)
+    for i in range(n):
+        p, s = posed(prim, pp[i], py[i], pz[i]), posed(sec, sp[i], sy[i], sz[i])
+        m_cpu = glue.mutual_inductance(p, s, args=args, method=0)
+        assert abs(m[i] - m_cpu) <= TOL * abs(m_cpu), (i, m[i], m_cpu)
+        ft_cpu = glue.force_torque(p, s, args=args, method=0)
+        # the coil-level force glue's correction factor is 2 pi N2 / I1 (not 2 pi N2 I2)
+        got = ft[i] * prim[4] * sec[4]
+        assert np.linalg.norm(got[:3] - ft_cpu[:3]) <= TOL * np.linalg.norm(ft_cpu[:3]), i
+        assert np.linalg.norm(got[3:] - ft_cpu[3:]) <= TOL * max(np.linalg.norm(ft_cpu[3:]), 1e-6 * np.linalg.norm(ft_cpu[:3])), i
+
+
+def test_group_arrangements(glue):
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(6, seed=41, centre_box=0.3)
+    sec = np.array([0.05, 0.02, 0.04, 80, 1.5, 50.0, 0, 0, 0, 0, 0])
+    n = 24
+    _, sp, _, _, sy, sz = arrangements(n, 22)
+    sp = sp + 0.15
+    m = glue.group_m_arrangements(rows, sec, sp, sy, sz, pf=5.0, method=GPU)
+    ft = glue.group_ft_arrangements(rows, sec, sp, sy, sz, pf=5.0, method=GPU)
+    half = (5.0 - 1.0) / 2.0 + 1.0  # the group GPU glue's PrecisionFactor
+    sargs = glue.secondary_precision_gpu(sec, half)
+    for i in range(n):
+        s = posed(sec, sp[i], sy[i], sz[i])
+        m_cpu, ft_cpu = 0.0, np.zeros(6)
+        for row in rows:
+            args = np.concatenate([glue.precision_args(row, half, gpu=True), sargs])
+            m_cpu += glue.mutual_inductance(row, s, args=args, method=0)
+            ft_cpu += glue.force_torque(row, s, args=args, method=0)
+        assert abs(m[i] - m_cpu) <= TOL * abs(m_cpu), (i, m[i], m_cpu)
+        assert np.linalg.norm(ft[i, :3] - ft_cpu[:3]) <= TOL * np.linalg.norm(ft_cpu[:3]), i
+        assert np.linalg.norm(ft[i, 3:] - ft_cpu[3:]) <= TOL * max(np.linalg.norm(ft_cpu[3:]), 1e-6 * np.linalg.norm(ft_cpu[:3])), i
