@@ -49,7 +49,7 @@ def parse():
                     help="coil-pair arrangements per GPU for the M and F/T part (0 skips it)")
     ap.add_argument("--cpu-sample-arrangements", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="group", choices=["group", "batched", "adjoint", "pf-sweep"],
+    ap.add_argument("--workload", default="group", choices=["group", "batched", "adjoint", "pf-sweep", "refine-sweep"],
                     help="group: the headline coil-group fields + pair arrangements; batched: many independent "
                          "systems in one persistent launch; adjoint: forward + backward of the B-field loss; "
                          "pf-sweep: the group at PrecisionFactor 1, 3, 5, 7, 9 (2^18 points)")
@@ -439,6 +439,70 @@ def bench_pf_sweep(a):
     print(json.dumps(line))
 
 
+def bench_refine_sweep(a):
+    """Cost curve of FP32_REFINED on the group workload: per field and refinement
+    ratio, the fraction of points re-evaluated in FP64, the time of the whole
+    evaluation and its error against FP64 (away from windings), beside plain
+    FP32_COMPENSATED and FP64."""
+    import ctypes
+    import torch
+    import ccoil_b200 as cc
+    from ccoil_b200 import workloads
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rows, _ = workloads.group_config(coils=a.coils, points=1)
+    coils = workloads.coils_from_rows(rows, a.pf)
+    group = cc.CoilGroup(coils, cc.PrecisionFactor(a.pf))
+    pts_host = workloads.points_cube(a.points, seed=1000 + 2)
+    pts = torch.from_numpy(pts_host).to(dev)
+    near, band = (torch.from_numpy(m).to(dev) for m in winding_masks(rows, pts_host))
+    flush = flush_l2(torch, dev)
+    L = cc.lib()
+    default_ratio = L.ccoil_refine_ratio()
+    ratios = [1.25, 1.5, 2.0, 3.0, 5.0, 10.0]
+
+    def timed(plan, out):
+        for _ in range(max(a.warmup, 1)):
+            plan(pts, out=out)
+        ms = 0.0
+        for _ in range(a.steps):
+            flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan(pts, out=out)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / a.steps
+
+    curve = {}
+    for name, f in FIELDS:
+        w = 9 if f == 3 else 3
+        away = ~band if f == 3 else ~near
+        outs = {}
+        res = {}
+        for label, mode in (("fp64", cc.PrecisionMode.FP64), ("fp32c", cc.PrecisionMode.FP32_COMPENSATED)):
+            plan = group.plan(f, mode)
+            outs[label] = torch.empty((a.points, w), dtype=torch.float64, device=dev)
+            res[label] = {"ms": timed(plan, outs[label])}
+            plan.close()
+        res["fp32c"]["err"] = rel_err_stats(outs["fp32c"], outs["fp64"], away)
+        for r in ratios:
+            L.ccoil_set_refine_ratio(ctypes.c_double(r))
+            plan = group.plan(f, cc.PrecisionMode.FP32_REFINED)
+            out = torch.empty((a.points, w), dtype=torch.float64, device=dev)
+            ms = timed(plan, out)
+            res["ratio_%g" % r] = {"ms": ms, "refined_fraction": plan.refined_points() / a.points,
+                                   "err": rel_err_stats(out, outs["fp64"], away),
+                                   "speedup_vs_fp64": res["fp64"]["ms"] / ms}
+            plan.close()
+        res["fp32c"]["speedup_vs_fp64"] = res["fp64"]["ms"] / res["fp32c"]["ms"]
+        curve[name] = res
+    L.ccoil_set_refine_ratio(ctypes.c_double(default_ratio))
+    print(json.dumps({"workload": "refine-sweep", "default_ratio": default_ratio, "config": workload_config(a, 1), "steps": a.steps,
+                      "l2": "flushed between timed evaluations", "curve": curve}))
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -452,6 +516,9 @@ def main():
         return
     if a.workload == "pf-sweep":
         bench_pf_sweep(a)
+        return
+    if a.workload == "refine-sweep":
+        bench_refine_sweep(a)
         return
 
     import torch
@@ -531,6 +598,18 @@ def main():
         results[int(mode)]["e2e_s"] = e2e_s
         for p in plans.values():
             p.close()
+        # one-shot calls, the reference glue's pattern (ccoil_compute_fields): every call
+        # builds and uploads the node tables, copies the points in and the results out
+        api = {"A": group.compute_all_A_potential_vectors, "B": group.compute_all_B_field_vectors,
+               "G": group.compute_all_B_gradient_matrices}
+        api["A"](pin_pts.numpy(), precision_mode=mode)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            for name, _f in FIELDS:
+                api[name](pin_pts.numpy(), precision_mode=mode)
+        results[int(mode)]["e2e_oneshot_s"] = max_over_ranks((time.perf_counter() - t0) / a.steps)
 
     units_per_step = len(FIELDS) * a.coils * a.points * world
     headline_mode = int(modes[-1])
@@ -538,36 +617,40 @@ def main():
     value = units_per_step / (r["step_ms"] * 1e-3)
     e2e_value = units_per_step / r["e2e_s"]
 
-    # roofline of the dominant kernel: its pipe work (opcount's model, divide /
-    # square root / log charged at their measured FP64-pipe cost) over its
-    # CUDA-event time, against the measured peak of the pipe that binds it
+    # roofline of the dominant kernel: its algorithmic work (the reference's operations
+    # per node, each add, multiply, divide, square root or logarithm one flop) over its
+    # CUDA-event time, against the measured FMA peak (2 flops per FMA) of the pipe it
+    # runs on; the instruction-issue and MUFU models are reported beside it
     rates = ctypes_rates(cc)
     dom = max(r["field_ms"], key=r["field_ms"].get)
     fidx = dict(FIELDS)[dom]
     t_dom = r["field_ms"][dom] * 1e-3
     flops_launch = opcount.group_flops_per_point(fidx, coils) * a.points
-    model = {"algorithmic_flops_per_launch": flops_launch, "algorithmic_tflops": flops_launch / t_dom / 1e12}
+    model = {"algorithmic_flops_per_launch": flops_launch}
     if rates is None:
         bound, achieved, peak, unit = "unmeasured", None, None, "TFLOP/s"
     elif headline_mode == 0:
-        slots = opcount.fp64_slots_per_point(fidx, coils, rates) * a.points
         bound, unit = "fp64-pipe", "TFLOP/s"
-        achieved, peak = 2.0 * slots / t_dom / 1e12, 2.0 * rates[0] / 1e12
-        model.update({"fp64_pipe_slots_per_launch": slots,
+        achieved, peak = flops_launch / t_dom / 1e12, 2.0 * rates[0] / 1e12
+        slots = opcount.fp64_slots_per_point(fidx, coils, rates) * a.points
+        model.update({"fp64_pipe_slots_per_launch": slots, "fp64_pipe_model_frac": slots / t_dom / rates[0],
                       "dfma_slots_per_op": {"div": rates[0] / rates[1], "sqrt": rates[0] / rates[2],
                                             "log": rates[0] / rates[3]}})
     else:
+        bound, unit = "fp32-pipe", "TFLOP/s"
+        achieved, peak = flops_launch / t_dom / 1e12, 2.0 * rates[4] / 1e12
         ins, mufu = opcount.fp32_ops_per_point(fidx, coils)
         ins, mufu = ins * a.points, mufu * a.points
-        issue, xu = ins / t_dom / rates[4], mufu / t_dom / rates[5]
-        if issue >= xu:
-            bound, unit = "fp32-issue", "TFLOP/s"
-            achieved, peak = 2.0 * ins / t_dom / 1e12, 2.0 * rates[4] / 1e12
-        else:
-            bound, unit = "xu (MUFU)", "Tops/s"
-            achieved, peak = mufu / t_dom / 1e12, rates[5] / 1e12
         model.update({"fp32_instructions_per_launch": ins, "mufu_ops_per_launch": mufu,
-                      "fp32_issue_frac": issue, "mufu_frac": xu})
+                      "fp32_issue_frac": ins / t_dom / rates[4], "mufu_frac": mufu / t_dom / rates[5]})
+    clk = r["clocks"] or {}
+    if clk.get("sm_mhz"):
+        # nominal B200 per-SM rates at the sampled clock: FP64 64 and FP32 128 FMA per clock,
+        # MUFU 16 per clock, 148 SMs
+        f = clk["sm_mhz"] * 1e6
+        model["nominal_at_sampled_clock"] = {"fp64_fma_tflops": 2 * 148 * 64 * f / 1e12,
+                                             "fp32_fma_tflops": 2 * 148 * 128 * f / 1e12,
+                                             "mufu_tops": 148 * 16 * f / 1e12, "sm_mhz": clk["sm_mhz"]}
     traffic = read_traffic(dom, headline_mode)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -582,10 +665,15 @@ def main():
             "clocks": r["clocks"],
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": len(FIELDS) * a.points * 24,
-                    "d2h_bytes_per_step": sum(a.points * 8 * (9 if f == 3 else 3) for _, f in FIELDS)},
+                    "d2h_bytes_per_step": sum(a.points * 8 * (9 if f == 3 else 3) for _, f in FIELDS),
+                    "path": "prepared plans (ccoil_field_plan_execute), pinned host points and results"},
+            "e2e_one_shot": {"value": units_per_step / r["e2e_oneshot_s"], "unit": UNIT,
+                             "path": "CoilGroup.compute_all_* (ccoil_compute_fields): node tables built and "
+                                     "uploaded, points copied in and results out on every call"},
             "roofline": {"bound": bound, "kernel": "field %s" % dom, "achieved": achieved, "peak": peak,
                          "unit": unit, "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                         "peak_source": "measured on this GPU by ccoil_measure_op_rates (FMA = 2 flops)",
+                         "peak_source": "measured on this GPU by ccoil_measure_op_rates (FMA = 2 flops); "
+                                        "achieved counts the reference's operations, one flop each",
                          "model": model,
                          "rates_measured": None if rates is None else {
                              "fp64_fma_tflops": 2 * rates[0] / 1e12, "fp32_fma_tflops": 2 * rates[4] / 1e12,

@@ -17,7 +17,7 @@ STATUS_NAMES = {
 }
 
 FIELD_A, FIELD_B, FIELD_E, FIELD_G = 0, 1, 2, 3
-PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
+PRECISION_FP64, PRECISION_FP32_COMPENSATED, PRECISION_FP32_REFINED = 0, 1, 2
 MEMORY_HOST, MEMORY_DEVICE = 0, 1
 
 
@@ -85,6 +85,11 @@ def lib():
     L.ccoil_field_plan_execute.argtypes = [vp, vp, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_int, vp]
     L.ccoil_field_plan_destroy.argtypes = [vp]
     L.ccoil_timeout_count.restype = ctypes.c_longlong
+    L.ccoil_check_bounded_wait.argtypes = [ctypes.c_longlong, vp]
+    L.ccoil_set_refine_ratio.argtypes = [ctypes.c_double]
+    L.ccoil_refine_ratio.restype = ctypes.c_double
+    L.ccoil_field_plan_refined_points.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.ccoil_inject_allocation_failures.argtypes = [ctypes.c_int]
     L.ccoil_batch_plan_create.argtypes = [cp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.ccoil_batch_plan_execute.argtypes = [vp, vp, vp, vp, vp, vp]

@@ -41,6 +41,7 @@ class PrecisionMode(enum.IntEnum):
     """Arithmetic of the quadrature (runtime choice; the reference fixes it with the TYPE macro)."""
     FP64 = _lib.PRECISION_FP64
     FP32_COMPENSATED = _lib.PRECISION_FP32_COMPENSATED
+    FP32_REFINED = _lib.PRECISION_FP32_REFINED
 
 
 class PrecisionFactor:
@@ -176,6 +177,12 @@ class FieldPlan:
                                              res.ctypes.data_as(ctypes.c_void_p), _lib.MEMORY_HOST, int(lanes),
                                              ctypes.c_void_p(stream or 0)))
         return res
+
+    def refined_points(self):
+        """Points the last execution re-evaluated in FP64 (FP32_REFINED plans)."""
+        n = ctypes.c_longlong()
+        check(lib().ccoil_field_plan_refined_points(self._h, ctypes.byref(n)))
+        return n.value
 
     def close(self):
         if self._h:

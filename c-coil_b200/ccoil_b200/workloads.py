@@ -109,9 +109,10 @@ def batched_config(groups=2048, seed=4, min_points=256, max_points=65536, max_gr
     return systems
 
 
-def adjoint_config(coils=64, points=4096, seed=5):
-    """64 RECTANGULAR coils (parameters as the group configuration), points in a ball of 5 cm."""
-    return coil_rows_mixed(coils, seed, types=[0]), points_ball(points, seed + 7)
+def adjoint_config(coils=64, points=4096, seed=5, types=(0,)):
+    """64 RECTANGULAR coils (parameters as the group configuration), points in a ball of 5 cm;
+    `types` cycles other coil types instead."""
+    return coil_rows_mixed(coils, seed, types=list(types)), points_ball(points, seed + 7)
 
 
 def coils_from_rows(rows, precision_factor=5.0):

@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -62,10 +64,20 @@ namespace
 std::mutex g_poolMutex;
 constexpr int kMaxDevices = 64;
 cudaMemPool_t g_pools[kMaxDevices] = {};
+// allocations still to fail on purpose (ccoil_inject_allocation_failures)
+std::atomic<int> g_failAllocations{0};
+// FP32_REFINED: re-evaluate a point in FP64 when the norms of its FP32
+// contributions add up to more than this ratio times the norm of its total
+std::atomic<double> g_refineRatio{kDefaultRefineRatio};
+// device-side wait timeouts already reported to a caller
+std::atomic<long long> g_timeoutsReported{0};
 } // namespace
 
 cudaError_t scratchAlloc(void **p, size_t bytes, cudaStream_t st)
 {
+    for (int n = g_failAllocations.load(); n > 0;)
+        if (g_failAllocations.compare_exchange_weak(n, n - 1))
+            return cudaErrorMemoryAllocation;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
@@ -144,6 +156,7 @@ struct ccoil_field_plan
     int coil_count = 0;
     SegmentSet set;
     DeviceBuffer blob, segs, points, out, work, workCount;
+    DeviceBuffer cabs, refine, refineCount;  // FP32_REFINED
 };
 
 extern "C" {
@@ -212,8 +225,9 @@ int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field
         return fail(CCOIL_ERR_INVALID_ARGUMENT, "coil_count < 0 or coils null");
     if (field < CCOIL_FIELD_A || field > CCOIL_FIELD_G)
         return fail(CCOIL_ERR_INVALID_ARGUMENT, "field must be A, B, E or G");
-    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
-        return fail(CCOIL_ERR_INVALID_ARGUMENT, "precision must be FP64 or FP32_COMPENSATED");
+    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED &&
+        precision != CCOIL_PRECISION_FP32_REFINED)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "precision must be FP64, FP32_COMPENSATED or FP32_REFINED");
 
     ccoil_field_plan *p = new (std::nothrow) ccoil_field_plan();
     if (!p)
@@ -222,7 +236,8 @@ int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field
     p->precision = precision;
     p->coil_count = coil_count;
     std::string err;
-    if (!buildFieldSegments(coils, coil_count, field, precision, p->set, err))
+    const int tables = precision == CCOIL_PRECISION_FP64 ? CCOIL_PRECISION_FP64 : CCOIL_PRECISION_FP32_COMPENSATED;
+    if (!buildFieldSegments(coils, coil_count, field, tables, p->set, err))
     {
         delete p;
         return fail(CCOIL_ERR_INVALID_ARGUMENT, err);
@@ -299,7 +314,7 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
     L.field = plan->field;
     L.precision = plan->precision;
     L.lanes = lanes_per_point ? lanes_per_point : autoLanes(point_count);
-    if (plan->precision == CCOIL_PRECISION_FP32_COMPENSATED)
+    if (plan->precision == CCOIL_PRECISION_FP32_COMPENSATED || plan->precision == CCOIL_PRECISION_FP32_REFINED)
     {
         // near-field work list: room for every (point, segment) pair up to 4 Mi
         // entries (32 MiB); pairs beyond it are integrated in FP64 in place
@@ -317,6 +332,22 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
         L.d_work_count = static_cast<unsigned long long *>(plan->workCount.ptr);
         L.near_blocks = 148 * 8;
     }
+    if (plan->precision == CCOIL_PRECISION_FP32_REFINED)
+    {
+        // every point can be listed: the list never overflows
+        int rc0 = plan->cabs.reserve(sizeof(double) * (size_t)point_count);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->refine.reserve(sizeof(int) * (size_t)point_count);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->refineCount.reserve(sizeof(unsigned long long));
+        if (rc0 != CCOIL_OK)
+            return rc0;
+        L.refine_ratio = g_refineRatio.load();
+        L.d_cabs = static_cast<double *>(plan->cabs.ptr);
+        L.d_refine = static_cast<int *>(plan->refine.ptr);
+        L.refine_capacity = plan->refine.bytes / sizeof(int);
+        L.d_refine_count = static_cast<unsigned long long *>(plan->refineCount.ptr);
+    }
     int rc = launchFields(L, stream);
     if (rc != CCOIL_OK)
         return rc;
@@ -332,10 +363,9 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
         rc = readTimeouts(timeouts);
         if (rc != CCOIL_OK)
             return rc;
-        static thread_local long long seen = 0;
-        if (timeouts > seen)
+        if (timeouts > g_timeoutsReported.load())
         {
-            seen = timeouts;
+            g_timeoutsReported.store(timeouts);
             return fail(CCOIL_ERR_TIMEOUT, "a staging wait in the field kernel timed out");
         }
     }
@@ -352,6 +382,9 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
     plan->out.release();
     plan->work.release();
     plan->workCount.release();
+    plan->cabs.release();
+    plan->refine.release();
+    plan->refineCount.release();
     delete plan;
     return CCOIL_OK;
 }
@@ -359,6 +392,11 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
 int ccoil_compute_fields(const ccoil_coil_t *coils, int coil_count, const double *points, long long point_count,
                          int field, int precision, double *out, int memory, void *stream)
 {
+    // the execute step's own checks, before any device work
+    if (point_count < 0 || (point_count > 0 && (!points || !out)))
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "point_count < 0 or null points/out");
+    if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
     ccoil_field_plan_t *plan = nullptr;
     int rc = ccoil_field_plan_create(coils, coil_count, field, precision, &plan);
     if (rc != CCOIL_OK)
@@ -373,6 +411,51 @@ int ccoil_compute_fields(const ccoil_coil_t *coils, int coil_count, const double
     }
     ccoil_field_plan_destroy(plan);
     return rc;
+}
+
+int ccoil_check_bounded_wait(long long limit_cycles, void *stream)
+{
+    if (limit_cycles < 0 || limit_cycles > 4000000000LL)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "limit_cycles must lie in [0, 4e9]");
+    const int rc = checkBoundedWait(limit_cycles, stream);
+    // this call reports its own timeout; field calls report only theirs
+    long long count = 0;
+    if (readTimeouts(count) == CCOIL_OK)
+        g_timeoutsReported.store(count);
+    return rc;
+}
+
+int ccoil_set_refine_ratio(double ratio)
+{
+    if (!(ratio >= 1.0) || !std::isfinite(ratio))
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "the refinement ratio must be finite and >= 1");
+    g_refineRatio.store(ratio);
+    return CCOIL_OK;
+}
+
+double ccoil_refine_ratio(void) { return g_refineRatio.load(); }
+
+int ccoil_field_plan_refined_points(ccoil_field_plan_t *plan, long long *count)
+{
+    if (!plan || !count)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "null plan or count");
+    *count = 0;
+    if (plan->precision != CCOIL_PRECISION_FP32_REFINED || !plan->refineCount.ptr)
+        return CCOIL_OK;
+    unsigned long long v = 0;
+    cudaError_t e = cudaMemcpy(&v, plan->refineCount.ptr, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cudaFail(e, "refinement count");
+    *count = (long long)v;
+    return CCOIL_OK;
+}
+
+int ccoil_inject_allocation_failures(int count)
+{
+    if (count < 0)
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "count < 0");
+    g_failAllocations.store(count);
+    return CCOIL_OK;
 }
 
 long long ccoil_timeout_count(void)

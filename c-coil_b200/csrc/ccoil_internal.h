@@ -60,17 +60,18 @@ struct SegmentDesc
 // FP32 angular tables, appended after the FP64 tables (16 bytes per entry).
 // One entry describes a mirror pair of nodes: node k of the first half of
 // [0, pi] and node n-1-k (phi -> pi - phi), whose cosine is the exact negation.
-// The FP32 integrands evaluate both nodes and accumulate w c (f(c) - f(-c)) and
-// w (g(c) + g(-c)): far from the coil the two values agree to many digits and
-// their difference is exact in FP32, so the accumulation carries only the
-// antisymmetric part and needs no compensation.  Both nodes are formed from
-// the same per-thickness-node constants (Q + b2 omc and Q + b2 omcm), so the
-// rounding of those constants is common to the pair and cancels in the
-// difference.  With an odd node count the middle node (c = 0) is an entry of
-// its own with half its weight (evaluated twice).
+// Every squared distance the integrands use is Q + b2 (1 - cos), so the second
+// node's exceed the first's by the same delta = b2 (omcm - omc) = 2 b2 c.  The
+// FP32 integrands form f(c) - f(-c) as delta times a cancellation-free
+// expression and g(c) + g(-c) directly; the entry carries
+// w2c2 = w (omcm - omc)^2 / 2 = 2 w c^2, the weight of such a difference divided
+// by b2, computed from the FP32 values of omc and omcm so that it matches the
+// distances the kernels form from them.  With an odd node count the middle
+// node (c = 0) is an entry of its own with half its weight (evaluated twice,
+// w2c2 = 0).
 struct alignas(16) PhiNode32
 {
-    float wc;    // w_phi * c, c = (cos(phi_k) - cos(phi_{n-1-k})) / 2 (0 for the middle node)
+    float w2c2;  // w (omcm - omc)^2 / 2 (0 for the middle node)
     float omc;   // 1 - cos(phi_k) = 2 sin^2(phi_k / 2)
     float omcm;  // 1 - cos(phi_{n-1-k}) = 2 sin^2(phi_{n-1-k} / 2) (about 2 - omc)
     float w;     // w_phi (halved for the middle node)
@@ -157,10 +158,20 @@ struct FieldLaunch
     unsigned long long work_capacity = 0;
     unsigned long long *d_work_count = nullptr;
     int near_blocks = 0;                    // grid of the near-field pass
+    // FP32_REFINED: points whose FP32 contributions' norms add up to more than
+    // refine_ratio times the norm of their total are re-evaluated in FP64
+    double refine_ratio = 0.0;              // 0: no refinement
+    double *d_cabs = nullptr;               // double[npts] (scratch)
+    int *d_refine = nullptr;                // int[refine_capacity] (scratch)
+    unsigned long long refine_capacity = 0;
+    unsigned long long *d_refine_count = nullptr;
 };
 constexpr size_t kNearPairBytes = 8;
+// default ratio of the FP32_REFINED test (ccoil_set_refine_ratio)
+constexpr double kDefaultRefineRatio = 4.0;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
+int checkBoundedWait(long long limitCycles, void *stream);
 
 // batched persistent launch (fields.cu, batch.cuh)
 struct BatchLaunch

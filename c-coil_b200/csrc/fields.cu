@@ -26,8 +26,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 namespace ccoil
 {
+int cudaFail(cudaError_t e, const char *what);
+
 namespace
 {
 __device__ unsigned long long g_timeouts = 0;
@@ -72,18 +76,36 @@ __device__ __forceinline__ bool mbarTryWait(unsigned long long *bar, unsigned pa
     return ok != 0;
 }
 
-// Bounded wait: returns false after ~2 s without completion.
-__device__ __forceinline__ bool mbarWait(unsigned long long *bar, unsigned parity)
+// Bounded wait: returns false after `limit` clock cycles (~2 s by default)
+// without completion.
+__device__ __forceinline__ bool mbarWait(unsigned long long *bar, unsigned parity, long long limit = kWaitCycles)
 {
     if (mbarTryWait(bar, parity))
         return true;
     long long start = clock64();
     while (!mbarTryWait(bar, parity))
     {
-        if (clock64() - start > kWaitCycles)
+        if (clock64() - start > limit)
             return false;
     }
     return true;
+}
+
+// Exercises the bounded wait on an mbarrier that nothing completes: one thread
+// initialises it for one arrival that never comes and waits at most `limit`
+// cycles; a wait that gives up is counted in g_timeouts and reported in *status
+// (1), and the kernel returns normally.  No copy is in flight on the barrier.
+__global__ void boundedWaitKernel(long long limit, int *status)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0)
+        return;
+    mbarInit(&bar, 1);
+    fenceBarrierInit();
+    const bool ok = mbarWait(&bar, 0, limit);
+    if (!ok)
+        atomicAdd(&g_timeouts, 1ull);
+    *status = ok ? 0 : 1;
 }
 
 #include "integrands64.cuh"
@@ -198,7 +220,9 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     long long blocks = (L.npts + ppb - 1) / ppb;
     if (blocks > 2147483647LL)
         return cudaErrorInvalidConfiguration;
-    const bool fp32 = L.precision == CCOIL_PRECISION_FP32_COMPENSATED;
+    const bool fp32 = L.precision == CCOIL_PRECISION_FP32_COMPENSATED || L.precision == CCOIL_PRECISION_FP32_REFINED;
+    const bool refine = fp32 && L.refine_ratio > 0.0 && L.d_cabs && L.d_refine && L.d_refine_count;
+    double *cabs = refine ? L.d_cabs : nullptr;
     const bool staged = fp32 ? CCOIL_FP32_STAGE : CCOIL_FP64_STAGE;
     const size_t smem = staged ? (size_t)kSegmentStages * kSegmentBytes : 0;
     NearPair *work = reinterpret_cast<NearPair *>(L.d_work);
@@ -208,7 +232,8 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     case N:                                                                                                       \
         if (fp32)                                                                                                 \
             fieldsKernel32<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(                                    \
-                L.d_blob, L.d_segs, L.nseg, L.d_points, L.npts, L.d_out, work, L.work_capacity, L.d_work_count);  \
+                L.d_blob, L.d_segs, L.nseg, L.d_points, L.npts, L.d_out, work, L.work_capacity, L.d_work_count,   \
+                cabs);                                                                                            \
         else                                                                                                      \
             fieldsKernel64<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(L.d_blob, L.d_segs, L.nseg,         \
                                                                               L.d_points, L.npts, L.d_out);       \
@@ -229,6 +254,15 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     // host synchronisation is needed between the passes
     nearFieldKernel<FIELD><<<L.near_blocks, 256, 0, st>>>(L.d_blob, L.d_segs, L.d_points, L.d_out, work,
                                                             L.work_capacity, L.d_work_count);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !refine)
+        return e;
+    constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
+    const long long testBlocks = std::min<long long>((L.npts + 255) / 256, 148LL * 16);
+    refineTestKernel<W><<<(unsigned)testBlocks, 256, 0, st>>>(L.d_out, L.d_cabs, L.npts, L.refine_ratio, L.d_refine,
+                                                             L.refine_capacity, L.d_refine_count);
+    refineKernel64<FIELD, 4><<<148 * 8, 128, 0, st>>>(L.d_blob, L.d_segs, L.nseg, L.d_points, L.d_out, L.d_refine,
+                                                     L.refine_capacity, L.d_refine_count);
     return cudaGetLastError();
 }
 } // namespace
@@ -245,13 +279,15 @@ int launchFields(const FieldLaunch &L, void *stream)
         return e == cudaSuccess ? CCOIL_OK : failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }
     cudaError_t e;
-    if (L.precision == CCOIL_PRECISION_FP32_COMPENSATED)
+    if (L.precision == CCOIL_PRECISION_FP32_COMPENSATED || L.precision == CCOIL_PRECISION_FP32_REFINED)
     {
         if (L.npts > 2147483647LL)
             return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED supports at most 2^31-1 points per call");
         if (!L.d_work || !L.d_work_count)
             return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED needs a near-field work list");
         e = cudaMemsetAsync(L.d_work_count, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess && L.d_refine_count)
+            e = cudaMemsetAsync(L.d_refine_count, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess)
             return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }
@@ -282,6 +318,26 @@ int batchBlocksPerSM(int precision)
                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                               &n, batchKernel<CCOIL_PRECISION_FP32_COMPENSATED>, 128, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+int checkBoundedWait(long long limitCycles, void *stream)
+{
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *dStatus = nullptr;
+    cudaError_t e = scratchAlloc(reinterpret_cast<void **>(&dStatus), sizeof(int), st);
+    if (e != cudaSuccess)
+        return cudaFail(e, "status word");
+    int status = 0;
+    boundedWaitKernel<<<1, 32, 0, st>>>(limitCycles, dStatus);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&status, dStatus, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(dStatus, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return cudaFail(e, "bounded wait");
+    return status ? fail(CCOIL_ERR_TIMEOUT, "the bounded wait gave up (nothing completed the barrier)") : CCOIL_OK;
 }
 
 int readTimeouts(long long &count)

@@ -10,8 +10,12 @@
 
 #include "integrands32.cuh"
 
+// Integrates one segment for one lane and returns the norm of the lane's
+// contribution (Frobenius norm for the gradient), taken from the cylindrical
+// partial sums before the rotation, which keeps it: the refinement test adds
+// these norms up per point.
 template <int FIELD, int LANES>
-__device__ __forceinline__ void integrateSegment32(const unsigned char *seg, const Frame &f, int lane, double *acc)
+__device__ __forceinline__ double integrateSegment32(const unsigned char *seg, const Frame &f, int lane, double *acc)
 {
     const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
     const double2 *tt = reinterpret_cast<const double2 *>(seg) + h.off_t;
@@ -22,17 +26,20 @@ __device__ __forceinline__ void integrateSegment32(const unsigned char *seg, con
         double H, Z;
         segmentB32<LANES>(h, tt, lt, pn, f, lane, H, Z);
         addRotated(h, H * f.cphi, H * f.sphi, Z, acc);
+        return sqrt(H * H + Z * Z);
     }
     else if (FIELD == CCOIL_FIELD_G)
     {
         double g[4];
         segmentG32<LANES>(h, tt, lt, pn, f, lane, g);
         addGradient(h, f, g, acc);
+        return sqrt(g[0] * g[0] + g[1] * g[1] + 2.0 * g[2] * g[2] + g[3] * g[3]);
     }
     else
     {
         double a = segmentA32<LANES>(h, tt, lt, pn, f, lane) * h.field_factor;
         addRotated(h, -a * f.sphi, a * f.cphi, 0.0, acc);
+        return fabs(a);
     }
 }
 
@@ -85,7 +92,8 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
                                                       const double *__restrict__ points, long long npts,
                                                       double *__restrict__ out, NearPair *__restrict__ work,
                                                       unsigned long long workCapacity,
-                                                      unsigned long long *__restrict__ workCount)
+                                                      unsigned long long *__restrict__ workCount,
+                                                      double *__restrict__ cabs)
 {
     constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -120,6 +128,7 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
 #pragma unroll
     for (int i = 0; i < W; ++i)
         acc[i] = 0.0;
+    double cn = 0.0;  // sum of the segments' contribution norms (refinement test)
 
     for (int s = 0; s < nseg; ++s)
     {
@@ -139,7 +148,7 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
             const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
             const Frame f = toCoilFrame(h, px, py, pz);
             if (!nearWinding(h, f))
-                integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
+                cn += integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
             else
             {
                 bool queued = false;
@@ -187,14 +196,19 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
 
 #pragma unroll
     for (int off = LANES / 2; off > 0; off /= 2)
+    {
 #pragma unroll
         for (int i = 0; i < W; ++i)
             acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+        cn += __shfl_xor_sync(0xffffffffu, cn, off);
+    }
     if (active && lane == 0)
     {
 #pragma unroll
         for (int i = 0; i < W; ++i)
             out[W * p + i] = acc[i];
+        if (cabs)
+            cabs[p] = cn;
     }
 }
 
@@ -234,6 +248,77 @@ __global__ void __launch_bounds__(256) nearFieldKernel(const unsigned char *__re
 #pragma unroll
             for (int k = 0; k < W; ++k)
                 atomicAdd(&out[W * p + k], acc[k]);
+        }
+    }
+}
+
+// Refinement test: a point whose FP32-evaluated contributions have norms that
+// add up to more than `ratio` times the norm of its total (the coils' fields
+// cancel there, and the total's relative error grows by that ratio; the
+// near-field pairs, evaluated in FP64, do not count) is listed for
+// re-evaluation in FP64.
+template <int W>
+__global__ void __launch_bounds__(256) refineTestKernel(const double *__restrict__ out,
+                                                        const double *__restrict__ cabs, long long npts, double ratio,
+                                                        int *__restrict__ list, unsigned long long capacity,
+                                                        unsigned long long *__restrict__ count)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npts;
+         p += (long long)gridDim.x * blockDim.x)
+    {
+        double n2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            n2 += out[W * p + k] * out[W * p + k];
+        // !(a <= b) also lists points whose values are not finite
+        if (!(cabs[p] <= ratio * sqrt(n2)))
+        {
+            const unsigned long long slot = atomicAdd(count, 1ull);
+            if (slot < capacity)
+                list[slot] = (int)p;
+        }
+    }
+}
+
+// FP64 re-evaluation of the listed points: all segments with the FP64
+// integrands, LANES threads per point splitting the angular nodes, the result
+// overwriting the point's output.  Grid-stride over the device-side count (no
+// host synchronisation between the passes); a list that overflowed leaves the
+// remaining points at their FP32 values, which the caller learns from the count.
+template <int FIELD, int LANES>
+__global__ void __launch_bounds__(128) refineKernel64(const unsigned char *__restrict__ blob,
+                                                      const SegmentDesc *__restrict__ segs, int nseg,
+                                                      const double *__restrict__ points, double *__restrict__ out,
+                                                      const int *__restrict__ list, unsigned long long capacity,
+                                                      const unsigned long long *__restrict__ count)
+{
+    constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
+    const unsigned long long n = min(*count, capacity);
+    const int lane = threadIdx.x % LANES;
+    const unsigned long long groups = (unsigned long long)gridDim.x * (blockDim.x / LANES);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * (blockDim.x / LANES) + threadIdx.x / LANES;
+         i < n; i += groups)
+    {
+        const long long p = list[i];
+        double acc[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            acc[k] = 0.0;
+        const double px = points[3 * p], py = points[3 * p + 1], pz = points[3 * p + 2];
+        for (int s = 0; s < nseg; ++s)
+            integrateSegment64<FIELD, LANES>(blob + segs[s].offset, px, py, pz, lane, acc);
+        const unsigned groupMask = LANES == 32 ? 0xffffffffu
+                                               : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
+#pragma unroll
+        for (int off = LANES / 2; off > 0; off /= 2)
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                acc[k] += __shfl_xor_sync(groupMask, acc[k], off);
+        if (lane == 0)
+        {
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                out[W * p + k] = acc[k];
         }
     }
 }

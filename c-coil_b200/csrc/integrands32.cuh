@@ -5,16 +5,18 @@
 // Arithmetic.  Per point and coil the frame transform, the per-thickness-node
 // constants and the final sums are FP64; the angular loop runs in FP32 over
 // mirror pairs of nodes (phi, pi - phi): each step evaluates both nodes and
-// adds w cos (f(c) - f(-c)) and w (g(c) + g(-c)) to FP32 running sums.
-// The cos-weighted sums cancel far from the coil; pairing cancels them inside
-// each step, where f(c) and f(-c) agree to many digits and their difference is
-// exact, so the running sums hold only the surviving part.  The vector
-// potential and the field still compensate their sums (Kahan: it halves their
-// 99th-percentile error); the gradient and the arrangement kernels add plainly
-// (their error is set elsewhere).  Both nodes of a pair take every quantity of the form
+// adds w c (f(c) - f(-c)) and w (g(c) + g(-c)) to FP32 running sums.
+// Far from the coil f(c) and f(-c) agree to many digits: the vector potential
+// and the field form their difference in closed form, as delta = 2 b2 c times a
+// cancellation-free expression (below), so its relative error does not grow
+// with the distance; the gradient subtracts (its error stays two orders below
+// the others').  The vector potential and the field compensate their sums
+// (Kahan: it halves their 99th-percentile error); the arrangement kernels add
+// plainly (the FP64 sum over the secondary's nodes averages their rounding).
+// Both nodes of a pair take every quantity of the form
 // Q + b2 (1 - cos) from the same FP32 constants Q and b2 (with their own
-// 1 - cos, omc and omcm), so the rounding of Q and b2 is common to the pair
-// and drops out of the difference.  The FP32 integrands are
+// 1 - cos, omc and omcm), so the rounding of Q and b2 is common to the pair.
+// The FP32 integrands are
 // algebraic rewrites of the reference's (CalculateFieldsFast.cxx,
 // CalculateFieldsSlow.cxx) that remove every cancellation FP32 cannot afford:
 //   distance^2     D - 2 p r cos  ->  (p - r)^2 + z^2 + 2 p r (1 - cos)
@@ -233,15 +235,15 @@ __device__ __forceinline__ float asinhAny(float u)
     return au < 1e18f ? asinhLarge(u) : asinhf(u);
 }
 
-// asinh(u) - asinh(v) for a mirror pair in a tier the warp chose beforehand:
-// 0 every lane's arguments below 0.25, 1 below 1, 2 per lane
-__device__ __forceinline__ float asinhDiffTier(float u, float v, int tier)
+// asinh(u) in a tier the warp chose beforehand: 0 every lane's argument below
+// 0.25, 1 below 1, 2 per lane
+__device__ __forceinline__ float asinhTier(float u, int tier)
 {
     if (tier == 0)
-        return asinhSmall(u) - asinhSmall(v);
+        return asinhSmall(u);
     if (tier == 1)
-        return asinhMid(u) - asinhMid(v);
-    return asinhAny(u) - asinhAny(v);
+        return asinhMid(u);
+    return asinhAny(u);
 }
 
 __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame &f)
@@ -249,6 +251,37 @@ __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame 
     return f.r > h.near_lo[0] && f.r < h.near_hi[0] && f.z > h.near_lo[1] && f.z < h.near_hi[1];
 }
 
+// Mirror-pair differences in closed form.  For the pair (c, -c) the second
+// node's squared distances exceed the first's by delta = b2 (omcm - omc); with
+// g = 1 / sqrt(D) and g' = 1 / sqrt(D + delta),
+//   g - g' = delta e,  e = g^2 g'^2 / (g + g'),
+// and every difference below is delta times a sum of terms of one sign, so its
+// relative error stays that of a few FP32 roundings however far the point is
+// (forming f(c) - f(-c) by subtraction loses the ratio distance / radius).
+// The accumulated weight of a difference is w2c2 = 2 w c^2 (= w c delta / b2),
+// so b2 multiplies the sums after the loop, in FP64.
+struct PairInv
+{
+    float i1, i2;  // 1 / (x1 + x1'), 1 / (x2 + x2') from one reciprocal
+};
+__device__ __forceinline__ PairInv pairInverse(float a, float b)
+{
+    const float r = rcpApprox(a * b);
+    return {b * r, a * r};
+}
+
+// Vector potential.  Fast method: per node asinh(u) with u = dD / (top s2 + bot s1)
+// outside the slab, (top s2 - bot s1) / rho^2 inside it (s the distances to the
+// slab's faces); the pair's difference is asinh(u) - asinh(u') =
+// asinh((u - u') (u + u') / (u sqrt(1 + u'^2) + u' sqrt(1 + u^2))), with u - u'
+// in closed form:
+//   outside  (u - u') / delta = dD (top / (s2 + s2') + bot / (s1 + s1')) / (V V'),  V = top s2 + bot s1
+//   inside   (u - u') / delta = [top (bot^2 + s2 s2') / (s2 + s2') - bot (top^2 + s1 s1') / (s1 + s1')]
+//                               / (rho^2 rho'^2)
+// (outside, top and bot share a sign; inside, top > 0 > bot, so every term is
+// positive).  u and u' share a sign, so the last denominator does not cancel
+// either.
+// Slow method: sum w c (g - g') = b2 sum w2c2 e.
 // S: the running-sum type of the pair accumulation (Kahan or PlainSum);
 // UNIFORM: warp-uniform slab branches (bySlab)
 template <int LANES, typename S = Kahan, bool UNIFORM = true>
@@ -262,35 +295,61 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
         const bool same = top * bot > 0.0;
         const float topf = (float)top, botf = (float)bot;
-        const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
+        const double dD = 2.0 * f.z * (2.0 * h.half_length);
+        const float dDf = (float)dD, dDl = (float)(dD - (double)dDf);
         bySlab<UNIFORM>(same, [&](auto slab) {
             const bool outside = slabOutside<decltype(slab)::value>(same);
-            // argument of the single asinh at one node from rho^2 and the two distances^2
-            auto arg = [&](float rho2, float den1, float den2) {
-                const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
-                const float a = topf * s2, b = botf * s1;
-                const float num = outside ? dDf : (a - b);
-                const float den = outside ? (a + b) : rho2;
-                return num * rcpApprox(den);
-            };
             for (int j = 0; j < h.n_t; ++j)
             {
                 const double2 t = tt[j];
                 const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
                 const float qf = (float)q, b2 = (float)b2d;
                 const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-                // |u| decreases with 1 - cos on either side of the slab, so its value
-                // at phi = 0 bounds every node of this thickness node: one warp vote
-                // picks the asinh form for all of them
-                const float u0 = fabsf(arg(qf, d1, d2));
+                // |u| decreases with 1 - cos on either side of the slab and the
+                // difference's argument stays below max(|u|, |u'|), so |u| at phi = 0
+                // bounds every argument of this thickness node: one warp vote picks the
+                // asinh form for all of them
+                float u0;
+                {
+                    const float e1 = d1 * rsqrtNR(d1), e2 = d2 * rsqrtNR(d2);
+                    u0 = outside ? fabsf(fmaf(dDl, 1.0f, dDf) * rcpApprox(fmaf(topf, e2, botf * e1)))
+                                 : fabsf(fmaf(topf, e2, -botf * e1) * rcpApprox(qf));
+                }
                 const unsigned mask = __activemask();
                 const int tier = __all_sync(mask, u0 < 0.25f) ? 0 : (__all_sync(mask, u0 <= 1.0f) ? 1 : 2);
                 Acc1<S> a0, a1;
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
                     const PhiNode32 nd = pn[k];
-                    const float u = arg(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2));
-                    const float um = arg(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2));
-                    acc.v.add(nd.wc * asinhDiffTier(u, um, tier));
+                    const float dom = nd.omcm - nd.omc;  // delta / b2
+                    const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
+                    const float den1m = fmaf(b2, nd.omcm, d1), den2m = fmaf(b2, nd.omcm, d2);
+                    const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
+                    const float s1m = den1m * rsqrtNR(den1m), s2m = den2m * rsqrtNR(den2m);
+                    const PairInv is = pairInverse(s1 + s1m, s2 + s2m);
+                    float u, um, du;
+                    if (outside)
+                    {
+                        const float v = fmaf(topf, s2, botf * s1), vm = fmaf(topf, s2m, botf * s1m);
+                        const PairInv iv = pairInverse(v, vm);
+                        u = fmaf(dDl, iv.i1, dDf * iv.i1);
+                        um = fmaf(dDl, iv.i2, dDf * iv.i2);
+                        du = fmaf(topf, is.i2, botf * is.i1) * (u * iv.i2);
+                    }
+                    else
+                    {
+                        const float rho2 = fmaf(b2, nd.omc, qf), rho2m = fmaf(b2, nd.omcm, qf);
+                        const PairInv ir = pairInverse(rho2, rho2m);
+                        u = fmaf(topf, s2, -botf * s1) * ir.i1;
+                        um = fmaf(topf, s2m, -botf * s1m) * ir.i2;
+                        // top (bot^2 + s2 s2') / (s2 + s2') - bot (top^2 + s1 s1') / (s1 + s1'), both terms >= 0
+                        du = fmaf(topf * fmaf(botf, botf, s2 * s2m), is.i2, -botf * fmaf(topf, topf, s1 * s1m) * is.i1) *
+                             (ir.i1 * ir.i2);
+                    }
+                    // sqrt(1 + u^2), sqrt(1 + u'^2)
+                    const float y = fmaf(u, u, 1.0f), ym = fmaf(um, um, 1.0f);
+                    const float sq = y * rsqrtNR(y), sqm = ym * rsqrtNR(ym);
+                    const float arg = (du * (b2 * dom)) * ((u + um) * rcpApprox(fmaf(u, sqm, um * sq)));
+                    acc.v.add((0.5f * nd.w * dom) * asinhTier(arg, tier));
                 });
                 sum += t.y * t.x * (a0.v.value() + a1.v.value());
             }
@@ -311,14 +370,36 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
                     const PhiNode32 nd = pn[k];
                     const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
-                    acc.v.add(nd.wc * (g - gm));
+                    const float gg = g * gm;
+                    acc.v.add(nd.w2c2 * (gg * gg * rcpApprox(g + gm)));
                 });
-                sum += l.y * t.y * t.x * (a0.v.value() + a1.v.value());
+                sum += l.y * t.y * t.x * (double)b2 * (a0.v.value() + a1.v.value());
             }
         }
     }
     return sum;
 }
+
+// Field.  Fast method, per node: the H integrand over dD w c is
+// hv = g1^2 g2^2 / (g1 + g2) and the Z integrand over w is num y with
+// num = p^2 - p r c and y = (top g1 - bot g2) / rho^2 (= dD g1^2 g2^2 / (top g1 + bot g2)
+// outside the slab; dD multiplies after the loop there).  The pair contributes
+//   H: w c (hv - hv') = b2 w2c2 kh,
+//      kh = (u1 + u2' + u1^2 / (u2 + u2') + u2'^2 / (u1 + u1')) hv hv'   (u = 1 / g)
+//   Z: w (num y + num' y') = w (2 p^2 y' + num (y - y')),  y - y' = delta ey:
+//      outside [top g1 g1' (e1 g2^2 + g1' e2 (g2 + g2')) + bot g2 g2' (e1 (g1 + g1') g2 + g1'^2 e2)] / (X X'),
+//              X = top g1 + bot g2
+//      inside  (top e1 - bot e2 + y') / rho^2.
+// Far from the coil, num y + num' y' subtracts two terms ~ p r c y; near the
+// winding (y >> y'), p^2 (y + y') - p r c (y - y') does; 2 p^2 y' + num (y - y')
+// does neither (num = p (p - r) + p r (1 - c) from the table).
+// Slow method: with k3 = (g^3 - g'^3) / delta = e (g^2 + g g' + g'^2),
+//   H: w c (g^3 - g'^3) = b2 w2c2 k3,   Z: w (2 p^2 g'^3 + num delta k3).
+template <typename S>
+struct Acc3
+{
+    S h, y, e;
+};
 
 template <int LANES, typename S = Kahan>
 __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
@@ -330,46 +411,55 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        const bool same = top * bot > 0.0;
+        const bool outside = top * bot > 0.0;  // per lane (slab branches measured no faster for B)
         const float topf = (float)top, botf = (float)bot;
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
-        const float dDf = (float)dD;
-        bySlab<false>(same, [&](auto slab) {  // per lane: branches measured no faster for B
-            const bool outside = slabOutside<decltype(slab)::value>(same);
-            // one node: hv (the H integrand over dD w c) and zv (the Z integrand over w)
-            auto node = [&](float rho2, float den1, float den2, float num, float &hv, float &zv) {
-                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
-                const float gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
-                const float t1 = topf * g1, t2 = botf * g2;
-                const float X = outside ? (t1 + t2) : rho2;
-                const float Y = outside ? dDf * gg2 : (t1 - t2);
-                const float R = rcpApprox(s * X);
-                hv = gg2 * (X * R);
-                zv = num * Y * (s * R);
-            };
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
-                const float qf = (float)q, b2 = (float)b2d;
-                const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-                // p^2 - p r cos = p (p - r) + p r (1 - cos)
-                const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-                Acc2<S> a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
-                    const PhiNode32 nd = pn[k];
-                    float hv, zv, hm, zm;
-                    node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), fmaf(n1, nd.omc, n0), hv,
-                         zv);
-                    node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), fmaf(n1, nd.omcm, n0),
-                         hm, zm);
-                    acc.h.add(nd.wc * (hv - hm));
-                    acc.z.add(nd.w * (zv + zm));
-                });
-                H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
-                Z += t.y * (a0.z.value() + a1.z.value());
-            }
-        });
+        const double zScale = outside ? dD : 1.0;
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+            const float qf = (float)q, b2 = (float)b2d;
+            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+            const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
+            Acc3<S> a0, a1;
+            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc3<S> &acc) {
+                const PhiNode32 nd = pn[k];
+                const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
+                const float den1m = fmaf(b2, nd.omcm, d1), den2m = fmaf(b2, nd.omcm, d2);
+                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2), g1m = rsqrtNR(den1m), g2m = rsqrtNR(den2m);
+                // per node: hv, y and 1 / X from one reciprocal of (g1 + g2) X
+                auto node = [&](float a, float b, float rho2, float &hv, float &y, float &ix) {
+                    const float gg = a * b, gg2 = gg * gg, s = a + b;
+                    const float t1 = topf * a, t2 = botf * b;
+                    const float X = outside ? t1 + t2 : rho2;
+                    const float R = rcpApprox(s * X);
+                    hv = gg2 * (X * R);
+                    ix = s * R;
+                    y = (outside ? gg2 : t1 - t2) * ix;
+                };
+                float hv, y, ix, hvm, ym, ixm;
+                node(g1, g2, fmaf(b2, nd.omc, qf), hv, y, ix);
+                node(g1m, g2m, fmaf(b2, nd.omcm, qf), hvm, ym, ixm);
+                const float s1 = g1 + g1m, s2 = g2 + g2m;
+                const PairInv is = pairInverse(s1, s2);
+                const float p1 = g1 * g1m, p2 = g2 * g2m;
+                const float e1 = p1 * p1 * is.i1, e2 = p2 * p2 * is.i2;
+                const float u1 = den1 * g1, u2m = den2m * g2m;
+                const float kh = ((u1 + u2m) + fmaf(u1 * u1, p2 * is.i2, (u2m * u2m) * (p1 * is.i1))) * (hv * hvm);
+                const float ey = outside ? fmaf(topf * p1, fmaf(e1, g2 * g2, g1m * (e2 * s2)),
+                                                botf * p2 * fmaf(e1 * s1, g2, g1m * g1m * e2)) *
+                                               (ix * ixm)
+                                         : (fmaf(topf, e1, -botf * e2) + ym) * ix;
+                const float num = fmaf(n1, nd.omc, n0);  // p^2 - p r c = p (p - r) + p r (1 - c)
+                acc.h.add(nd.w2c2 * kh);
+                acc.y.add(nd.w * ym);
+                acc.e.add((nd.w * (nd.omcm - nd.omc)) * (num * ey));
+            });
+            const double b2f = (double)b2;
+            H += t.y * t.x * dD * b2f * (a0.h.value() + a1.h.value());
+            Z += t.y * zScale * (2.0 * t.x * t.x * (a0.y.value() + a1.y.value()) + b2f * (a0.e.value() + a1.e.value()));
+        }
     }
     else
     {
@@ -383,17 +473,20 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
                 const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
                 const float qf = (float)q, b2 = (float)b2d;
                 const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-                Acc2<S> a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc2<S> &acc) {
+                Acc3<S> a0, a1;
+                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc3<S> &acc) {
                     const PhiNode32 nd = pn[k];
                     const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
-                    const float g3 = g * g * g, g3m = gm * gm * gm;
-                    acc.z.add(nd.w * fmaf(g3, fmaf(n1, nd.omc, n0), g3m * fmaf(n1, nd.omcm, n0)));
-                    acc.h.add(nd.wc * (g3 - g3m));
+                    const float gg = g * gm, g2 = g * g, gm2 = gm * gm;
+                    const float k3 = gg * gg * rcpApprox(g + gm) * (g2 + fmaf(g, gm, gm2));
+                    const float num = fmaf(n1, nd.omc, n0);
+                    acc.h.add(nd.w2c2 * k3);
+                    acc.y.add(nd.w * (gm2 * gm));
+                    acc.e.add((nd.w * (nd.omcm - nd.omc)) * (num * k3));
                 });
-                const double w = l.y * t.y;
-                H += w * t.x * zl * (a0.h.value() + a1.h.value());
-                Z += w * (a0.z.value() + a1.z.value());
+                const double w = l.y * t.y, b2f = (double)b2;
+                H += w * t.x * zl * b2f * (a0.h.value() + a1.h.value());
+                Z += w * (2.0 * t.x * t.x * (a0.y.value() + a1.y.value()) + b2f * (a0.e.value() + a1.e.value()));
             }
         }
     }
@@ -448,14 +541,15 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 Acc4 a0, a1;
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
                     const PhiNode32 nd = pn[k];
+                    const float wc = 0.5f * nd.w * (nd.omcm - nd.omc);
                     float dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
                     node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), dg, dg3, cz, kz);
                     node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), dgm, dg3m, czm, kzm);
                     const float sin2 = hb2 * (nd.omc * nd.omcm);  // p r sin^2 = (b2 / 2)(1 - c)(1 + c)
-                    acc.a = fmaf(nd.wc, dg - dgm, acc.a);
-                    acc.b = fmaf(nd.wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
+                    acc.a = fmaf(wc, dg - dgm, acc.a);
+                    acc.b = fmaf(wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
                     acc.d = fmaf(nd.w, fmaf(fmaf(rf, nd.omc, pmr), dg3, fmaf(rf, nd.omcm, pmr) * dg3m), acc.d);
-                    acc.c = fmaf(nd.wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
+                    acc.c = fmaf(wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
                 });
                 const double w = t.y * t.x;
                 rphi += w / r * ((double)a0.a + (double)a1.a);
@@ -486,14 +580,15 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 Acc4 a0, a1;
                 forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
                     const PhiNode32 nd = pn[k];
+                    const float wc = 0.5f * nd.w * (nd.omcm - nd.omc);
                     const float den = fmaf(b2, nd.omc, qf), denm = fmaf(b2, nd.omcm, qf);
                     const float gq = rsqrtNR(den), gqm = rsqrtNR(denm);
                     const float g3 = gq * gq * gq, g5 = g3 * gq * gq;
                     const float g3m = gqm * gqm * gqm, g5m = g3m * gqm * gqm;
                     const float rpc = fmaf(pf, nd.omc, rmp), prc = fmaf(rf, nd.omc, pmr);
                     const float rpcm = fmaf(pf, nd.omcm, rmp), prcm = fmaf(rf, nd.omcm, pmr);
-                    acc.a = fmaf(nd.wc, g3 - g3m, acc.a);
-                    acc.b = fmaf(nd.wc, fmaf(g5, rpc, -g5m * rpcm), acc.b);
+                    acc.a = fmaf(wc, g3 - g3m, acc.a);
+                    acc.b = fmaf(wc, fmaf(g5, rpc, -g5m * rpcm), acc.b);
                     acc.d = fmaf(nd.w, fmaf(g5, prc, g5m * prcm), acc.d);
                     acc.c = fmaf(nd.w, fmaf(g5 * prc, rpc, g5m * prcm * rpcm), acc.c);
                 });

@@ -47,11 +47,11 @@ void appendBytes(std::vector<unsigned char> &blob, const void *p, size_t n)
 } // namespace
 
 // Entry k of the FP32 angular pair table: node k of the FP64 table (in the
-// reference's order) and its mirror n-1-k.  The weighted cosine takes the
-// symmetric definition (cos(phi_k) - cos(phi_m)) / 2, so the mirror's is its
-// exact negation; both nodes' 1 - cos come from half-angle sines (no
-// cancellation near phi = 0 or pi); an odd table's middle node is an entry of
-// its own with half its weight.
+// reference's order) and its mirror n-1-k.  Both nodes' 1 - cos come from
+// half-angle sines (no cancellation near phi = 0 or pi); the difference weight
+// w2c2 is formed from their FP32 values, so it matches the squared distances
+// the kernels build from them; an odd table's middle node is an entry of its
+// own with half its weight.
 PhiNode32 phiPair32(const PrecisionArgs &p, int k)
 {
     const double aBlock = kPi / p.angular_blocks;
@@ -68,13 +68,14 @@ PhiNode32 phiPair32(const PrecisionArgs &p, int k)
     if (m == k)
     {
         e.omcm = e.omc;
-        e.wc = 0.0f;
+        e.w2c2 = 0.0f;
         e.w = (float)(0.5 * w);
     }
     else
     {
         e.omcm = (float)(2.0 * sm * sm);
-        e.wc = (float)(w * 0.5 * (std::cos(phiOf(k)) - std::cos(phiOf(m))));
+        const double twoC = (double)e.omcm - (double)e.omc;
+        e.w2c2 = (float)(0.5 * w * twoC * twoC);
         e.w = (float)w;
     }
     return e;

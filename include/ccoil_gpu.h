@@ -48,11 +48,17 @@ typedef enum ccoil_status
 
 /* Arithmetic of the quadrature.  FP64 reproduces the reference's double CPU
  * path; FP32_COMPENSATED runs the bulk of the nodes in FP32 with compensated
- * accumulation and keeps FP64 for near-field points and the final sums. */
+ * accumulation and keeps FP64 for near-field points and the final sums;
+ * FP32_REFINED (fields) is FP32_COMPENSATED followed by an FP64 re-evaluation
+ * of every point where the coils' fields cancel, i.e. where the norms of the
+ * FP32-evaluated contributions add up to more than a set ratio times the norm
+ * of the total (ccoil_set_refine_ratio; the total's relative error grows by
+ * that ratio). */
 typedef enum ccoil_precision
 {
     CCOIL_PRECISION_FP64 = 0,
-    CCOIL_PRECISION_FP32_COMPENSATED = 1
+    CCOIL_PRECISION_FP32_COMPENSATED = 1,
+    CCOIL_PRECISION_FP32_REFINED = 2
 } ccoil_precision_t;
 
 typedef enum ccoil_field
@@ -162,6 +168,15 @@ int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field
 int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, long long point_count, double *out,
                              int memory, int lanes_per_point, void *stream);
 int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
+
+/* FP32_REFINED's test ratio (process-wide, read when a plan executes; >= 1):
+ * a point is re-evaluated in FP64 when the norms of its FP32-evaluated
+ * contributions add up to more than `ratio` times the norm of its total.
+ * Smaller ratios refine more points.  ccoil_field_plan_refined_points reports
+ * how many points the plan's last execution re-evaluated (synchronous). */
+int ccoil_set_refine_ratio(double ratio);
+double ccoil_refine_ratio(void);
+int ccoil_field_plan_refined_points(ccoil_field_plan_t *plan, long long *count);
 
 /* ------------------------------------------------------------------------ *
  * Coil pairs over many arrangements                                         *
@@ -305,6 +320,20 @@ int ccoil_b_field_adjoint(const double *params, const ccoil_precision_args_t *pr
  * bounded waits of the staging pipeline; a non-zero value also makes the
  * failing call return CCOIL_ERR_TIMEOUT). */
 long long ccoil_timeout_count(void);
+
+/* Failure-path checks, no counterpart in the reference (whose CUDA error path
+ * ends the process, src/CUDAUtils/ErrorCheck/ErrorCheck.cu:15).
+ * ccoil_check_bounded_wait runs the staging pipeline's bounded mbarrier wait on
+ * a barrier that nothing completes, for at most limit_cycles GPU clock cycles
+ * (<= 4e9, about 2 s): it returns CCOIL_ERR_TIMEOUT, counts the timeout in
+ * ccoil_timeout_count(), and leaves the context usable.  Synchronous on
+ * `stream`.
+ * ccoil_inject_allocation_failures makes the next `count` device allocations
+ * of the library's memory pool fail (as out of memory), so a caller can check
+ * that its calls return CCOIL_ERR_OUT_OF_MEMORY and that later calls work;
+ * count = 0 clears it. */
+int ccoil_check_bounded_wait(long long limit_cycles, void *stream);
+int ccoil_inject_allocation_failures(int count);
 
 /* FP32_COMPENSATED field evaluation that allocates nothing.  No counterpart in
  * the reference.  For callers that cannot allocate device memory: plugins

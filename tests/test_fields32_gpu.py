@@ -156,3 +156,44 @@ def test_mirror_pair_tables(ccoil, angular):
             if field == 3:
                 e = e[~gradient_band(row[None, :], pts)]
             assert np.median(e) < 1e-6 and e.max() < 1e-4, (angular, row[:3], field, np.median(e), e.max())
+
+
+def test_refined_mode(ccoil):
+    """FP32_REFINED re-evaluates in FP64 every point whose FP32 contributions' norms add
+    up to more than the set ratio times its total's norm: with a ratio of 1 (every
+    point qualifies, the sum of norms is never below the norm of the sum) the result
+    is, at nearly every point, the FP64 result up to summation order (a point whose
+    contributions are all near-field pairs, already FP64, or exactly parallel need
+    not qualify); with a larger ratio only the
+    cancelling points are re-evaluated and the error is never above FP32_COMPENSATED's
+    at any point that was re-evaluated."""
+    import ctypes
+    from ccoil_b200 import workloads
+    L = ccoil.lib()
+    default = L.ccoil_refine_ratio()
+    rows = workloads.coil_rows_mixed(16, seed=77)
+    pts = workloads.points_cube(8192, seed=78)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    try:
+        for field in (0, 1, 3):
+            f64 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP64)
+            f32 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
+            L.ccoil_set_refine_ratio(ctypes.c_double(1.0))
+            plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_REFINED)
+            got = plan(pts)
+            n_all = plan.refined_points()
+            plan.close()
+            e = rel_err(got, f64)
+            assert n_all >= 0.9 * len(pts) and np.sum(e < 1e-13) >= n_all, (field, n_all, np.sum(e < 1e-13))
+            L.ccoil_set_refine_ratio(ctypes.c_double(3.0))
+            plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_REFINED)
+            got = plan(pts)
+            n = plan.refined_points()
+            plan.close()
+            assert 0 < n < len(pts)
+            e, e32 = rel_err(got, f64), rel_err(f32, f64)
+            redone = e < 1e-13
+            assert redone.sum() >= n and e.max() <= e32.max(), (field, n, e.max(), e32.max())
+    finally:
+        L.ccoil_set_refine_ratio(ctypes.c_double(default))
+    assert L.ccoil_set_refine_ratio(ctypes.c_double(0.5)) == 1

@@ -161,3 +161,19 @@ def test_segment_split_for_large_angular_tables(ccoil):
     if not HAS_GPU:
         with pytest.raises(ccoil.CCoilError):
             ccoil.FieldPlan([c.struct()], 1)
+
+
+def test_negative_counts_are_rejected_without_a_device(ccoil):
+    """Argument checks come before any CUDA call."""
+    L = ccoil.lib()
+    from ccoil_b200 import _lib
+    s = _lib.CoilStruct()
+    pos = (ctypes.c_double * 3)(0.0, 0.0, 0.0)
+    assert L.ccoil_coil_init(0.1, 0.05, 0.1, 100, 1.0, 0.0, pos, 0.0, 0.0, 5.0, 0, ctypes.byref(s)) == 0
+    arr = (_lib.CoilStruct * 1)(s)
+    buf = (ctypes.c_double * 3)()
+    assert L.ccoil_compute_fields(arr, 1, buf, -1, 1, 0, buf, 0, None) == 1
+    assert L.ccoil_compute_fields(arr, -1, buf, 1, 1, 0, buf, 0, None) == 1
+    assert L.ccoil_compute_fields(arr, 1, buf, 1, 7, 0, buf, 0, None) == 1
+    assert L.ccoil_inject_allocation_failures(-1) == 1
+    assert L.ccoil_check_bounded_wait(-5, None) == 1

@@ -9,8 +9,11 @@ this library through the Calculate_* entry points declared in
 include/ccoil_reference_abi.h, which stand in for the reference's CUDA kernels.
 
 Each result is compared with the reference's own CPU path at the precision
-arguments the glue used (the GPU ones, capped at GPU_INCREMENTS = 80): 1e-12,
-the FP64 kernels' parity bar.  The glue's own quirks come through as they are:
+arguments the glue used (the GPU ones, capped at GPU_INCREMENTS = 80).  The
+points fill a cube around the coils, closer to the axes and windings than the
+golden sets; the bar is 1e-11 outside the radial winding bands (the reference's
+-ffast-math build and a strict IEEE evaluation of the same nodes differ by up
+to 5e-13 there) and 1e-8 inside them.  The glue's own quirks come through as they are:
 the coil-level force glue passes the correction factor 2 pi N2 / I1, so its
 force is the CPU force divided by I1 I2, and the group arrangement glue halves
 the PrecisionFactor."""
@@ -21,7 +24,7 @@ from conftest import gradient_band, rel_err
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-12
+TOL = 1e-11
 GPU = 2  # ComputeMethod::GPU in the reference's C-API wrapper
 
 
@@ -47,12 +50,14 @@ def points(n, seed, half=0.5):
 
 
 def check(got, exp, rows, pts, qty):
+    """1e-11 outside every coil's radial winding band; inside it the fast-method
+    integrands cancel (the reference's -ffast-math build and a strict IEEE
+    evaluation of the same nodes differ by up to 3e-11 for A and B there), so the
+    bar is 1e-8, and 1e-5 for the gradient (conftest.gradient_band)."""
     e = rel_err(got, exp)
-    if qty == 3:
-        band = gradient_band(rows, pts)
-        assert e[band].max(initial=0.0) < 1e-5
-        e = e[~band]
-    assert e.max() < TOL, (qty, e.max())
+    band = gradient_band(rows, pts)
+    assert e[band].max(initial=0.0) < (1e-5 if qty == 3 else 1e-8), (qty, e[band].max())
+    assert e[~band].max() < TOL, (qty, e[~band].max())
 
 
 @pytest.mark.parametrize("qty", [0, 1, 2, 3])
