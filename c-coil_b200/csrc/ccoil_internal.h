@@ -77,6 +77,18 @@ struct alignas(16) PhiNode32
     float w;     // w_phi (halved for the middle node)
 };
 
+// Device layout of the FP32 angular table: two consecutive mirror pairs per
+// 32-byte entry, every field a float2 {pair 2m, pair 2m + 1}, so the integrands
+// evaluate both pairs with packed FP32 (f32x2) instructions.  A table with an
+// odd pair count ends in an entry whose second pair has zero weights and the
+// first pair's nodes (its values stay finite and add nothing).
+struct alignas(16) PhiPair2
+{
+    float2 omc, omcm, w, w2c2;
+};
+static_assert(sizeof(PhiPair2) == 32, "FP32 angular entries are 32 bytes");
+void packPhiPairs2(const PhiNode32 *pairs, int count, std::vector<PhiPair2> &out);
+
 // Node order of the FP64 angular table in FP32 mode: position j holds node
 // j/2 (j even) or its mirror n-1-j/2 (j odd), so that any even-length slice of
 // the table covers whole mirror pairs; with odd n the middle node comes last.

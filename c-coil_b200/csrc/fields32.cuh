@@ -20,7 +20,7 @@ __device__ __forceinline__ double integrateSegment32(const unsigned char *seg, c
     const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
     const double2 *tt = reinterpret_cast<const double2 *>(seg) + h.off_t;
     const double2 *lt = reinterpret_cast<const double2 *>(seg) + h.off_l;
-    const PhiNode32 *pn = reinterpret_cast<const PhiNode32 *>(seg) + h.off_f32;
+    const PhiPair2 *pn = reinterpret_cast<const PhiPair2 *>(reinterpret_cast<const double2 *>(seg) + h.off_f32);
     if (FIELD == CCOIL_FIELD_B)
     {
         double H, Z;
@@ -59,15 +59,15 @@ struct NearPair
     int segment;
 };
 
-// CTAs per SM the register allocation targets, measured best on B200 over
-// 4-8 (2^20 points, 128-coil group): 6 for the vector potential, 5 for B,
-// 4 for the gradient (124 registers, no spills: 3.5 % faster than 5 CTAs
-// with 96 registers and spills; 3 CTAs was no faster)
+// CTAs per SM the register allocation targets (128 threads each): the packed
+// FP32 integrands hold two mirror pairs per value, and these are the highest
+// occupancies at which they compile without spills -- 5 for the vector
+// potential (96 registers), 4 for the field and the gradient (128 registers)
 #ifndef CCOIL_FP32_MIN_BLOCKS_A
-#define CCOIL_FP32_MIN_BLOCKS_A 6
+#define CCOIL_FP32_MIN_BLOCKS_A 5
 #endif
 #ifndef CCOIL_FP32_MIN_BLOCKS_B
-#define CCOIL_FP32_MIN_BLOCKS_B 5
+#define CCOIL_FP32_MIN_BLOCKS_B 4
 #endif
 #ifndef CCOIL_FP32_MIN_BLOCKS_G
 #define CCOIL_FP32_MIN_BLOCKS_G 4

@@ -32,14 +32,15 @@
 //                     reference's (p / M^2)(top L1 (O J1 + N) - bot L2 (O J2 + N)),
 //                     via N = c rho^4 - p r s^2 rho^2 and O = c rho^2 - 2 p r s^2,
 //                     without its 1/rho^4 cancellation
-// and the azimuthal tables hold one entry per mirror pair (PhiNode32).
+// and the azimuthal tables hold two mirror pairs per entry (PhiPair2).
 
 
-// Runs body(k, accumulator set) over the pair entries lane, lane + LANES, ...,
-// alternating between two independent accumulator sets so consecutive entries
-// do not wait on each other's additions (and each running sum stays short).
+// Runs body(j, accumulator set) over the packed entries (two mirror pairs each)
+// lane, lane + LANES, ..., alternating between two independent accumulator
+// sets so consecutive entries do not wait on each other's additions (and each
+// running sum stays short).
 template <int LANES, typename Acc, typename Body>
-__device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body body)
+__device__ __forceinline__ void forEntries(int n, int lane, Acc &a0, Acc &a1, Body body)
 {
     int k = lane;
     for (; k + LANES < n; k += 2 * LANES)
@@ -51,8 +52,9 @@ __device__ __forceinline__ void forNodes(int n, int lane, Acc &a0, Acc &a1, Body
         body(k, a0);
 }
 
-// pair entries of a table slice holding n angular nodes
-__device__ __forceinline__ int pairEntries(int n) { return (n + 1) >> 1; }
+// packed entries of a table slice holding n angular nodes: (n + 1) / 2 mirror
+// pairs, two per entry
+__device__ __forceinline__ int packedEntries(int n) { return (((n + 1) >> 1) + 1) >> 1; }
 
 // Fast method: whether a point lies outside the coil's length slab (|z| > b/2)
 // picks between two cancellation-free forms of each integrand.  When every
@@ -63,9 +65,8 @@ struct SlabTag
 {
     static constexpr int value = V;
 };
-// UNIFORM false: always the per-lane form (B, measured no faster with the
-// branches, and the arrangement kernels, whose out-of-line quadrature measured
-// 35 % slower with the three loop copies).
+// UNIFORM false: always the per-lane form (the arrangement kernels, whose
+// out-of-line quadrature measured 35 % slower with the three loop copies)
 template <bool UNIFORM, typename Loop>
 __device__ __forceinline__ void bySlab(bool outside, Loop loop)
 {
@@ -88,29 +89,53 @@ __device__ __forceinline__ bool slabOutside(bool perLane)
     return SLAB == 1 ? true : (SLAB == 2 ? false : perLane);
 }
 
-// Compensated (Kahan) running sum
+// Packed FP32 arithmetic (sm_100: add/sub/mul/fma.rn.f32x2, one instruction
+// for two lanes of a float2); every value of the angular loops is a float2
+// holding the same quantity for the two mirror pairs of a packed entry.
+using V2 = float2;
+__device__ __forceinline__ V2 v2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ V2 operator+(V2 a, V2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ V2 operator*(V2 a, V2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ V2 operator-(V2 a, V2 b)
+{
+    unsigned long long ra, rb, rr;
+    memcpy(&ra, &a, 8);
+    memcpy(&rb, &b, 8);
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rr) : "l"(ra), "l"(rb));
+    V2 r;
+    memcpy(&r, &rr, 8);
+    return r;
+}
+__device__ __forceinline__ V2 fma2(V2 a, V2 b, V2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ V2 sel(bool c, V2 a, V2 b) { return c ? a : b; }
+
+// Compensated (Kahan) running sums of both pairs of an entry; value() is
+// their FP64 total
 struct Kahan
 {
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x)
+    V2 s = {0.0f, 0.0f}, c = {0.0f, 0.0f};
+    __device__ __forceinline__ void add(V2 x)
     {
-        float y = x - c;
-        float t = s + y;
+        const V2 y = x - c;
+        const V2 t = s + y;
         c = (t - s) - y;
         s = t;
     }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+    __device__ __forceinline__ double value() const
+    {
+        return ((double)s.x - (double)c.x) + ((double)s.y - (double)c.y);
+    }
 };
 
-// Plain running sum, for callers whose error is set elsewhere (the gradient,
+// Plain running sums, for callers whose error is set elsewhere (the gradient,
 // whose pair sums stay far below the FP32 path's error bar, and the
 // arrangement kernels, whose FP64 sum over the secondary's nodes averages the
 // per-node rounding)
 struct PlainSum
 {
-    float s = 0.0f;
-    __device__ __forceinline__ void add(float x) { s += x; }
-    __device__ __forceinline__ double value() const { return (double)s; }
+    V2 s = {0.0f, 0.0f};
+    __device__ __forceinline__ void add(V2 x) { s = s + x; }
+    __device__ __forceinline__ double value() const { return (double)s.x + (double)s.y; }
 };
 
 template <typename S>
@@ -119,14 +144,15 @@ struct Acc1
     S v;
 };
 template <typename S>
-struct Acc2
+struct Acc3
 {
-    S h, z;
+    S h, y, e;
 };
 struct Acc4
 {
-    float a = 0.0f, b = 0.0f, c = 0.0f, d = 0.0f;
+    V2 a = {0.0f, 0.0f}, b = {0.0f, 0.0f}, c = {0.0f, 0.0f}, d = {0.0f, 0.0f};
 };
+__device__ __forceinline__ double hsum(V2 a) { return (double)a.x + (double)a.y; }
 
 // reciprocal: MUFU estimate (within 1 ulp), no special-case handling needed
 // since every argument here is a positive normal number
@@ -235,20 +261,67 @@ __device__ __forceinline__ float asinhAny(float u)
     return au < 1e18f ? asinhLarge(u) : asinhf(u);
 }
 
-// asinh(u) in a tier the warp chose beforehand: 0 every lane's argument below
-// 0.25, 1 below 1, 2 per lane
-__device__ __forceinline__ float asinhTier(float u, int tier)
-{
-    if (tier == 0)
-        return asinhSmall(u);
-    if (tier == 1)
-        return asinhMid(u);
-    return asinhAny(u);
-}
-
 __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame &f)
 {
     return f.r > h.near_lo[0] && f.r < h.near_hi[0] && f.z > h.near_lo[1] && f.z < h.near_hi[1];
+}
+
+__device__ __forceinline__ V2 rcp2(V2 x) { return make_float2(rcpApprox(x.x), rcpApprox(x.y)); }
+__device__ __forceinline__ V2 rsq2(V2 x) { return make_float2(rsqrtNR(x.x), rsqrtNR(x.y)); }
+
+// asinh of both lanes in a tier the warp chose beforehand: 0 every argument
+// below 0.25, 1 below 1, 2 per lane (the series and the polynomial packed)
+__device__ __forceinline__ V2 asinhTier2(V2 u, int tier)
+{
+    if (tier == 0)
+    {
+        const V2 u2 = u * u;
+        V2 p = v2(0.017352764f);
+        p = fma2(p, u2, v2(-0.022372159f));
+        p = fma2(p, u2, v2(0.030381944f));
+        p = fma2(p, u2, v2(-0.044642857f));
+        p = fma2(p, u2, v2(0.075f));
+        p = fma2(p, u2, v2(-0.16666667f));
+        return fma2(p * u2, u, u);
+    }
+    if (tier == 1)
+    {
+        const V2 x = u * u;
+        V2 p = v2(6.495655980e-04f);
+        p = fma2(p, x, v2(-3.737240797e-03f));
+        p = fma2(p, x, v2(1.025899500e-02f));
+        p = fma2(p, x, v2(-1.902823150e-02f));
+        p = fma2(p, x, v2(2.937856875e-02f));
+        p = fma2(p, x, v2(-4.446590319e-02f));
+        p = fma2(p, x, v2(7.498393208e-02f));
+        p = fma2(p, x, v2(-1.666660905e-01f));
+        p = fma2(p, x, v2(1.0f));
+        return u * p;
+    }
+    return make_float2(asinhAny(u.x), asinhAny(u.y));
+}
+
+// sqrt(1 + x) for 0 <= x < 1/16: 1 + x/2 - x^2/8 + x^3/16 - 5 x^4/128 + 7 x^5/256 - 21 x^6/1024
+__device__ __forceinline__ V2 sqrt1pSeries(V2 x)
+{
+    V2 p = v2(-0.0205078125f);
+    p = fma2(p, x, v2(0.02734375f));
+    p = fma2(p, x, v2(-0.0390625f));
+    p = fma2(p, x, v2(0.0625f));
+    p = fma2(p, x, v2(-0.125f));
+    p = fma2(p, x, v2(0.5f));
+    return fma2(p, x, v2(1.0f));
+}
+
+// 1 / a and 1 / b from one reciprocal
+struct PairInv
+{
+    V2 i1, i2;
+};
+__device__ __forceinline__ PairInv pairInverse(V2 a, V2 b)
+{
+    const V2 r = rcp2(a * b);
+    return {b * r, a * r};
 }
 
 // Mirror-pair differences in closed form.  For the pair (c, -c) the second
@@ -259,16 +332,8 @@ __device__ __forceinline__ bool nearWinding(const SegmentHeader &h, const Frame 
 // relative error stays that of a few FP32 roundings however far the point is
 // (forming f(c) - f(-c) by subtraction loses the ratio distance / radius).
 // The accumulated weight of a difference is w2c2 = 2 w c^2 (= w c delta / b2),
-// so b2 multiplies the sums after the loop, in FP64.
-struct PairInv
-{
-    float i1, i2;  // 1 / (x1 + x1'), 1 / (x2 + x2') from one reciprocal
-};
-__device__ __forceinline__ PairInv pairInverse(float a, float b)
-{
-    const float r = rcpApprox(a * b);
-    return {b * r, a * r};
-}
+// so b2 multiplies the sums after the loop, in FP64.  Every quantity is a
+// float2 over the two pairs of a packed entry.
 
 // Vector potential.  Fast method: per node asinh(u) with u = dD / (top s2 + bot s1)
 // outside the slab, (top s2 - bot s1) / rho^2 inside it (s the distances to the
@@ -286,10 +351,10 @@ __device__ __forceinline__ PairInv pairInverse(float a, float b)
 // UNIFORM: warp-uniform slab branches (bySlab)
 template <int LANES, typename S = Kahan, bool UNIFORM = true>
 __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                             const PhiNode32 *pn, const Frame &f, int lane)
+                                             const PhiPair2 *pn, const Frame &f, int lane)
 {
     double sum = 0.0;
-    const int np = pairEntries(h.n_phi);
+    const int ne = packedEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
@@ -297,6 +362,7 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
         const float topf = (float)top, botf = (float)bot;
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
         const float dDf = (float)dD, dDl = (float)(dD - (double)dDf);
+        const V2 TOP = v2(topf), BOT = v2(botf), NBOT = v2(-botf), DDF = v2(dDf), DDL = v2(dDl);
         bySlab<UNIFORM>(same, [&](auto slab) {
             const bool outside = slabOutside<decltype(slab)::value>(same);
             for (int j = 0; j < h.n_t; ++j)
@@ -317,39 +383,54 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
                 }
                 const unsigned mask = __activemask();
                 const int tier = __all_sync(mask, u0 < 0.25f) ? 0 : (__all_sync(mask, u0 <= 1.0f) ? 1 : 2);
+                const V2 B2 = v2(b2), D1 = v2(d1), D2 = v2(d2), Q = v2(qf);
                 Acc1<S> a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float dom = nd.omcm - nd.omc;  // delta / b2
-                    const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
-                    const float den1m = fmaf(b2, nd.omcm, d1), den2m = fmaf(b2, nd.omcm, d2);
-                    const float s1 = den1 * rsqrtNR(den1), s2 = den2 * rsqrtNR(den2);
-                    const float s1m = den1m * rsqrtNR(den1m), s2m = den2m * rsqrtNR(den2m);
-                    const PairInv is = pairInverse(s1 + s1m, s2 + s2m);
-                    float u, um, du;
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc1<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 dom = nd.omcm - nd.omc;  // delta / b2
+                    const V2 den1 = fma2(B2, nd.omc, D1), den2 = fma2(B2, nd.omc, D2);
+                    const V2 den1m = fma2(B2, nd.omcm, D1), den2m = fma2(B2, nd.omcm, D2);
+                    const V2 s1 = den1 * rsq2(den1), s2 = den2 * rsq2(den2);
+                    const V2 s1m = den1m * rsq2(den1m), s2m = den2m * rsq2(den2m);
+                    const V2 ss1 = s1 + s1m, ss2 = s2 + s2m;
+                    // 1 / (s1 + s1'), 1 / (s2 + s2') and 1 / V, 1 / V' (outside; inside the
+                    // slab 1 / rho^2, 1 / rho'^2) from one reciprocal of the four
+                    const V2 va = outside ? fma2(TOP, s2, BOT * s1) : fma2(B2, nd.omc, Q);
+                    const V2 vb = outside ? fma2(TOP, s2m, BOT * s1m) : fma2(B2, nd.omcm, Q);
+                    const V2 sp = ss1 * ss2, vp = va * vb;
+                    const V2 r = rcp2(sp * vp);
+                    const V2 rs = vp * r, rv = sp * r;  // 1 / (ss1 ss2), 1 / (va vb)
+                    const PairInv is = {ss2 * rs, ss1 * rs}, iv = {vb * rv, va * rv};
+                    V2 u, um, du;
                     if (outside)
                     {
-                        const float v = fmaf(topf, s2, botf * s1), vm = fmaf(topf, s2m, botf * s1m);
-                        const PairInv iv = pairInverse(v, vm);
-                        u = fmaf(dDl, iv.i1, dDf * iv.i1);
-                        um = fmaf(dDl, iv.i2, dDf * iv.i2);
-                        du = fmaf(topf, is.i2, botf * is.i1) * (u * iv.i2);
+                        u = fma2(DDL, iv.i1, DDF * iv.i1);
+                        um = fma2(DDL, iv.i2, DDF * iv.i2);
+                        du = fma2(TOP, is.i2, BOT * is.i1) * (u * iv.i2);
                     }
                     else
                     {
-                        const float rho2 = fmaf(b2, nd.omc, qf), rho2m = fmaf(b2, nd.omcm, qf);
-                        const PairInv ir = pairInverse(rho2, rho2m);
-                        u = fmaf(topf, s2, -botf * s1) * ir.i1;
-                        um = fmaf(topf, s2m, -botf * s1m) * ir.i2;
+                        u = fma2(TOP, s2, NBOT * s1) * iv.i1;
+                        um = fma2(TOP, s2m, NBOT * s1m) * iv.i2;
                         // top (bot^2 + s2 s2') / (s2 + s2') - bot (top^2 + s1 s1') / (s1 + s1'), both terms >= 0
-                        du = fmaf(topf * fmaf(botf, botf, s2 * s2m), is.i2, -botf * fmaf(topf, topf, s1 * s1m) * is.i1) *
-                             (ir.i1 * ir.i2);
+                        du = fma2(TOP * fma2(BOT, BOT, s2 * s2m), is.i2, NBOT * fma2(TOP, TOP, s1 * s1m) * is.i1) * rv;
                     }
-                    // sqrt(1 + u^2), sqrt(1 + u'^2)
-                    const float y = fmaf(u, u, 1.0f), ym = fmaf(um, um, 1.0f);
-                    const float sq = y * rsqrtNR(y), sqm = ym * rsqrtNR(ym);
-                    const float arg = (du * (b2 * dom)) * ((u + um) * rcpApprox(fmaf(u, sqm, um * sq)));
-                    acc.v.add((0.5f * nd.w * dom) * asinhTier(arg, tier));
+                    // sqrt(1 + u^2), sqrt(1 + u'^2): in tier 0 (|u| < 0.25) the binomial
+                    // series through x^6 (x = u^2, truncation below 1e-10), otherwise MUFU
+                    V2 sq, sqm;
+                    if (tier == 0)
+                    {
+                        sq = sqrt1pSeries(u * u);
+                        sqm = sqrt1pSeries(um * um);
+                    }
+                    else
+                    {
+                        const V2 y = fma2(u, u, v2(1.0f)), ym = fma2(um, um, v2(1.0f));
+                        sq = y * rsq2(y);
+                        sqm = ym * rsq2(ym);
+                    }
+                    const V2 arg = (du * (B2 * dom)) * ((u + um) * rcp2(fma2(u, sqm, um * sq)));
+                    acc.v.add((v2(0.5f) * nd.w * dom) * asinhTier2(arg, tier));
                 });
                 sum += t.y * t.x * (a0.v.value() + a1.v.value());
             }
@@ -365,13 +446,14 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
             {
                 const double2 t = tt[j];
                 const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
-                const float qf = (float)q, b2 = (float)b2d;
+                const float b2 = (float)b2d;
+                const V2 B2 = v2(b2), Q = v2((float)q);
                 Acc1<S> a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc1<S> &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
-                    const float gg = g * gm;
-                    acc.v.add(nd.w2c2 * (gg * gg * rcpApprox(g + gm)));
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc1<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 g = rsq2(fma2(B2, nd.omc, Q)), gm = rsq2(fma2(B2, nd.omcm, Q));
+                    const V2 gg = g * gm;
+                    acc.v.add(nd.w2c2 * (gg * gg * rcp2(g + gm)));
                 });
                 sum += l.y * t.y * t.x * (double)b2 * (a0.v.value() + a1.v.value());
             }
@@ -395,71 +477,71 @@ __device__ __forceinline__ double segmentA32(const SegmentHeader &h, const doubl
 // does neither (num = p (p - r) + p r (1 - c) from the table).
 // Slow method: with k3 = (g^3 - g'^3) / delta = e (g^2 + g g' + g'^2),
 //   H: w c (g^3 - g'^3) = b2 w2c2 k3,   Z: w (2 p^2 g'^3 + num delta k3).
-template <typename S>
-struct Acc3
-{
-    S h, y, e;
-};
-
-template <int LANES, typename S = Kahan>
+template <int LANES, typename S = Kahan, bool UNIFORM = true>
 __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                           const PhiNode32 *pn, const Frame &f, int lane, double &H, double &Z)
+                                           const PhiPair2 *pn, const Frame &f, int lane, double &H, double &Z)
 {
     H = 0.0;
     Z = 0.0;
-    const int np = pairEntries(h.n_phi);
+    const int ne = packedEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        const bool outside = top * bot > 0.0;  // per lane (slab branches measured no faster for B)
+        const bool same = top * bot > 0.0;
         const float topf = (float)top, botf = (float)bot;
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
-        const double zScale = outside ? dD : 1.0;
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
-            const float qf = (float)q, b2 = (float)b2d;
-            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-            const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
-            Acc3<S> a0, a1;
-            forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc3<S> &acc) {
-                const PhiNode32 nd = pn[k];
-                const float den1 = fmaf(b2, nd.omc, d1), den2 = fmaf(b2, nd.omc, d2);
-                const float den1m = fmaf(b2, nd.omcm, d1), den2m = fmaf(b2, nd.omcm, d2);
-                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2), g1m = rsqrtNR(den1m), g2m = rsqrtNR(den2m);
-                // per node: hv, y and 1 / X from one reciprocal of (g1 + g2) X
-                auto node = [&](float a, float b, float rho2, float &hv, float &y, float &ix) {
-                    const float gg = a * b, gg2 = gg * gg, s = a + b;
-                    const float t1 = topf * a, t2 = botf * b;
-                    const float X = outside ? t1 + t2 : rho2;
-                    const float R = rcpApprox(s * X);
-                    hv = gg2 * (X * R);
-                    ix = s * R;
-                    y = (outside ? gg2 : t1 - t2) * ix;
-                };
-                float hv, y, ix, hvm, ym, ixm;
-                node(g1, g2, fmaf(b2, nd.omc, qf), hv, y, ix);
-                node(g1m, g2m, fmaf(b2, nd.omcm, qf), hvm, ym, ixm);
-                const float s1 = g1 + g1m, s2 = g2 + g2m;
-                const PairInv is = pairInverse(s1, s2);
-                const float p1 = g1 * g1m, p2 = g2 * g2m;
-                const float e1 = p1 * p1 * is.i1, e2 = p2 * p2 * is.i2;
-                const float u1 = den1 * g1, u2m = den2m * g2m;
-                const float kh = ((u1 + u2m) + fmaf(u1 * u1, p2 * is.i2, (u2m * u2m) * (p1 * is.i1))) * (hv * hvm);
-                const float ey = outside ? fmaf(topf * p1, fmaf(e1, g2 * g2, g1m * (e2 * s2)),
-                                                botf * p2 * fmaf(e1 * s1, g2, g1m * g1m * e2)) *
-                                               (ix * ixm)
-                                         : (fmaf(topf, e1, -botf * e2) + ym) * ix;
-                const float num = fmaf(n1, nd.omc, n0);  // p^2 - p r c = p (p - r) + p r (1 - c)
-                acc.h.add(nd.w2c2 * kh);
-                acc.y.add(nd.w * ym);
-                acc.e.add((nd.w * (nd.omcm - nd.omc)) * (num * ey));
-            });
-            const double b2f = (double)b2;
-            H += t.y * t.x * dD * b2f * (a0.h.value() + a1.h.value());
-            Z += t.y * zScale * (2.0 * t.x * t.x * (a0.y.value() + a1.y.value()) + b2f * (a0.e.value() + a1.e.value()));
-        }
+        const V2 TOP = v2(topf), BOT = v2(botf), NBOT = v2(-botf);
+        bySlab<UNIFORM>(same, [&](auto slab) {
+            const bool outside = slabOutside<decltype(slab)::value>(same);
+            const double zScale = outside ? dD : 1.0;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+                const float b2 = (float)b2d;
+                const V2 B2 = v2(b2), Q = v2((float)q), D1 = v2((float)(top * top + q)),
+                         D2 = v2((float)(bot * bot + q));
+                const V2 N0 = v2((float)(t.x * (t.x - f.r))), N1 = v2((float)(t.x * f.r));
+                Acc3<S> a0, a1;
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc3<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 den1 = fma2(B2, nd.omc, D1), den2 = fma2(B2, nd.omc, D2);
+                    const V2 den1m = fma2(B2, nd.omcm, D1), den2m = fma2(B2, nd.omcm, D2);
+                    const V2 g1 = rsq2(den1), g2 = rsq2(den2), g1m = rsq2(den1m), g2m = rsq2(den2m);
+                    // per node: hv = g1^2 g2^2 / (g1 + g2), y, and 1 / X, all from 1 / ((g1 + g2) X)
+                    const V2 s = g1 + g2, sm = g1m + g2m;
+                    const V2 t1 = TOP * g1, t2 = BOT * g2, t1m = TOP * g1m, t2m = BOT * g2m;
+                    const V2 X = sel(outside, t1 + t2, fma2(B2, nd.omc, Q));
+                    const V2 Xm = sel(outside, t1m + t2m, fma2(B2, nd.omcm, Q));
+                    const V2 s1 = g1 + g1m, s2 = g2 + g2m;
+                    // one reciprocal for the three products (sX, sX', s1 s2)
+                    const V2 sx = s * X, sxm = sm * Xm, s12 = s1 * s2, sxx = sx * sxm;
+                    const V2 rr = rcp2(sxx * s12);
+                    const V2 R = (sxm * s12) * rr, Rm = (sx * s12) * rr, rc = sxx * rr;
+                    const V2 gg = g1 * g2, gg2 = gg * gg, ggm = g1m * g2m, gg2m = ggm * ggm;
+                    const V2 hv = gg2 * (X * R), hvm = gg2m * (Xm * Rm);
+                    const V2 ix = s * R, ixm = sm * Rm;
+                    const V2 y = sel(outside, gg2, t1 - t2) * ix, ym = sel(outside, gg2m, t1m - t2m) * ixm;
+                    const PairInv is = {s2 * rc, s1 * rc};
+                    const V2 p1 = g1 * g1m, p2 = g2 * g2m;
+                    const V2 e1 = p1 * p1 * is.i1, e2 = p2 * p2 * is.i2;
+                    const V2 u1 = den1 * g1, u2m = den2m * g2m;
+                    const V2 kh = ((u1 + u2m) + fma2(u1 * u1, p2 * is.i2, (u2m * u2m) * (p1 * is.i1))) * (hv * hvm);
+                    const V2 ey = outside ? fma2(TOP * p1, fma2(e1, g2 * g2, g1m * (e2 * s2)),
+                                                 BOT * p2 * fma2(e1 * s1, g2, g1m * g1m * e2)) *
+                                                (ix * ixm)
+                                          : (fma2(TOP, e1, NBOT * e2) + ym) * ix;
+                    const V2 num = fma2(N1, nd.omc, N0);  // p^2 - p r c = p (p - r) + p r (1 - c)
+                    acc.h.add(nd.w2c2 * kh);
+                    acc.y.add(nd.w * ym);
+                    acc.e.add((nd.w * (nd.omcm - nd.omc)) * (num * ey));
+                });
+                const double b2f = (double)b2;
+                H += t.y * t.x * dD * b2f * (a0.h.value() + a1.h.value());
+                Z += t.y * zScale *
+                     (2.0 * t.x * t.x * (a0.y.value() + a1.y.value()) + b2f * (a0.e.value() + a1.e.value()));
+            }
+        });
     }
     else
     {
@@ -471,15 +553,16 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
             {
                 const double2 t = tt[j];
                 const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
-                const float qf = (float)q, b2 = (float)b2d;
-                const float n0 = (float)(t.x * (t.x - f.r)), n1 = (float)(t.x * f.r);
+                const float b2 = (float)b2d;
+                const V2 B2 = v2(b2), Q = v2((float)q);
+                const V2 N0 = v2((float)(t.x * (t.x - f.r))), N1 = v2((float)(t.x * f.r));
                 Acc3<S> a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc3<S> &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float g = rsqrtNR(fmaf(b2, nd.omc, qf)), gm = rsqrtNR(fmaf(b2, nd.omcm, qf));
-                    const float gg = g * gm, g2 = g * g, gm2 = gm * gm;
-                    const float k3 = gg * gg * rcpApprox(g + gm) * (g2 + fmaf(g, gm, gm2));
-                    const float num = fmaf(n1, nd.omc, n0);
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc3<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 g = rsq2(fma2(B2, nd.omc, Q)), gm = rsq2(fma2(B2, nd.omcm, Q));
+                    const V2 gg = g * gm, g2 = g * g, gm2 = gm * gm;
+                    const V2 k3 = gg * gg * rcp2(g + gm) * (g2 + fma2(g, gm, gm2));
+                    const V2 num = fma2(N1, nd.omc, N0);
                     acc.h.add(nd.w2c2 * k3);
                     acc.y.add(nd.w * (gm2 * gm));
                     acc.e.add((nd.w * (nd.omcm - nd.omc)) * (num * k3));
@@ -495,18 +578,19 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
 // {RPhi, RR, RZ, ZZ}
 template <int LANES>
 __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                           const PhiNode32 *pn, const Frame &f, int lane, double *g)
+                                           const PhiPair2 *pn, const Frame &f, int lane, double *g)
 {
     double rphi = 0.0, rr = 0.0, rz = 0.0, zz = 0.0;
     const double r = f.r;
-    const int np = pairEntries(h.n_phi);
+    const int ne = packedEntries(h.n_phi);
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
         const bool same = top * bot > 0.0;
         const float topf = (float)top, botf = (float)bot, lenf = (float)(2.0 * h.half_length);
         const double dD = 2.0 * f.z * (2.0 * h.half_length);
-        const float dDf = (float)dD;
+        const V2 TOP = v2(topf), BOT = v2(botf), NBOT = v2(-botf), LEN = v2(lenf), DDF = v2((float)dD),
+                 NDDF = v2(-(float)dD);
         bySlab<true>(same, [&](auto slab) {
             const bool outside = slabOutside<decltype(slab)::value>(same);
             // one node: dg = G2 - G1, dg3 = G1^3 - G2^3, cz = T1 + Y (the RZ part
@@ -514,48 +598,52 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
             // the same for both nodes of a pair).  T1 = top G1^3 - bot G2^3 and
             // Y = (top G1 - bot G2) / rho^2, each in its cancellation-free form for a
             // point outside / inside the slab
-            auto node = [&](float rho2, float den1, float den2, float &dg, float &dg3, float &cz, float &kz) {
-                const float g1 = rsqrtNR(den1), g2 = rsqrtNR(den2);
-                const float gg = g1 * g2, s = g1 + g2;
-                const float ddgg = dDf * gg * gg;
-                dg = ddgg * rcpApprox(s);
-                dg3 = -dg * fmaf(g1, g1, fmaf(g1, g2, g2 * g2));
-                const float g13 = g1 * g1 * g1;
-                const float T1 = outside ? fmaf(lenf, g13, botf * dg3) : fmaf(topf, g13, -botf * (g2 * g2 * g2));
-                const float t1 = topf * g1, t2 = botf * g2;
-                const float yn = outside ? ddgg : (t1 - t2);
-                const float yd = outside ? (t1 + t2) : rho2;
-                const float Y = yn * rcpApprox(yd);
+            auto node = [&](V2 rho2, V2 den1, V2 den2, V2 &dg, V2 &dg3, V2 &cz, V2 &kz) {
+                const V2 g1 = rsq2(den1), g2 = rsq2(den2);
+                const V2 gg = g1 * g2, s = g1 + g2;
+                const V2 t1 = TOP * g1, t2 = BOT * g2;
+                const V2 yd = sel(outside, t1 + t2, rho2);
+                // 1 / s, 1 / yd and 1 / rho^2 from one reciprocal of their product
+                const V2 sy = s * yd, r = rcp2(sy * rho2);
+                const V2 rs = (yd * rho2) * r, ryd = (s * rho2) * r, rrho = sy * r;
+                const V2 gg2 = gg * gg, ggs = gg2 * rs;
+                const V2 ddgg = DDF * gg2;
+                dg = DDF * ggs;
+                dg3 = (NDDF * ggs) * fma2(g1, g1, fma2(g1, g2, g2 * g2));
+                const V2 g13 = g1 * g1 * g1;
+                const V2 T1 = outside ? fma2(LEN, g13, BOT * dg3) : fma2(TOP, g13, NBOT * (g2 * g2 * g2));
+                const V2 yn = sel(outside, ddgg, t1 - t2);
+                const V2 Y = yn * ryd;
                 cz = T1 + Y;
-                kz = fmaf(2.0f, Y, T1) * rcpApprox(rho2);
+                kz = fma2(v2(2.0f), Y, T1) * rrho;
             };
             for (int j = 0; j < h.n_t; ++j)
             {
                 const double2 t = tt[j];
                 const double q = (t.x - r) * (t.x - r), b2d = 2.0 * t.x * r;
-                const float qf = (float)q, b2 = (float)b2d, hb2 = (float)(0.5 * b2d);
-                const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
-                const float pf = (float)t.x, rf = (float)r;
+                const V2 B2 = v2((float)b2d), NHB2 = v2(-(float)(0.5 * b2d)), Q = v2((float)q);
+                const V2 D1 = v2((float)(top * top + q)), D2 = v2((float)(bot * bot + q));
+                const V2 PF = v2((float)t.x), NPF = v2(-(float)t.x), RF = v2((float)r);
                 // (r - p cos) = (r - p) + p (1 - cos); likewise (p - r cos)
-                const float rmp = (float)(r - t.x), pmr = (float)(t.x - r);
+                const V2 RMP = v2((float)(r - t.x)), NRMP = v2(-(float)(r - t.x)), PMR = v2((float)(t.x - r));
                 Acc4 a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float wc = 0.5f * nd.w * (nd.omcm - nd.omc);
-                    float dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
-                    node(fmaf(b2, nd.omc, qf), fmaf(b2, nd.omc, d1), fmaf(b2, nd.omc, d2), dg, dg3, cz, kz);
-                    node(fmaf(b2, nd.omcm, qf), fmaf(b2, nd.omcm, d1), fmaf(b2, nd.omcm, d2), dgm, dg3m, czm, kzm);
-                    const float sin2 = hb2 * (nd.omc * nd.omcm);  // p r sin^2 = (b2 / 2)(1 - c)(1 + c)
-                    acc.a = fmaf(wc, dg - dgm, acc.a);
-                    acc.b = fmaf(wc, fmaf(fmaf(pf, nd.omc, rmp), dg3, -fmaf(pf, nd.omcm, rmp) * dg3m), acc.b);
-                    acc.d = fmaf(nd.w, fmaf(fmaf(rf, nd.omc, pmr), dg3, fmaf(rf, nd.omcm, pmr) * dg3m), acc.d);
-                    acc.c = fmaf(wc, cz - czm, fmaf(-nd.w * sin2, kz + kzm, acc.c));
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc4 &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                    V2 dg, dg3, cz, kz, dgm, dg3m, czm, kzm;
+                    node(fma2(B2, nd.omc, Q), fma2(B2, nd.omc, D1), fma2(B2, nd.omc, D2), dg, dg3, cz, kz);
+                    node(fma2(B2, nd.omcm, Q), fma2(B2, nd.omcm, D1), fma2(B2, nd.omcm, D2), dgm, dg3m, czm, kzm);
+                    const V2 nsin2 = NHB2 * (nd.omc * nd.omcm);  // -p r sin^2 = -(b2 / 2)(1 - c)(1 + c)
+                    acc.a = fma2(wc, dg - dgm, acc.a);
+                    acc.b = fma2(wc, fma2(fma2(PF, nd.omc, RMP), dg3, fma2(NPF, nd.omcm, NRMP) * dg3m), acc.b);
+                    acc.d = fma2(nd.w, fma2(fma2(RF, nd.omc, PMR), dg3, fma2(RF, nd.omcm, PMR) * dg3m), acc.d);
+                    acc.c = fma2(wc, cz - czm, fma2(nd.w * nsin2, kz + kzm, acc.c));
                 });
                 const double w = t.y * t.x;
-                rphi += w / r * ((double)a0.a + (double)a1.a);
-                rr += w * ((double)a0.b + (double)a1.b);
-                zz += w * ((double)a0.d + (double)a1.d);
-                rz += w * ((double)a0.c + (double)a1.c);
+                rphi += w / r * (hsum(a0.a) + hsum(a1.a));
+                rr += w * (hsum(a0.b) + hsum(a1.b));
+                zz += w * (hsum(a0.d) + hsum(a1.d));
+                rz += w * (hsum(a0.c) + hsum(a1.c));
             }
         });
     }
@@ -570,33 +658,32 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 const double2 t = tt[j];
                 const double p = t.x;
                 const double q = (p - r) * (p - r) + zl * zl, b2d = 2.0 * p * r;
-                const float qf = (float)q, b2 = (float)b2d;
-                const float pf = (float)p, rf = (float)r;
-                const float rmp = (float)(r - p), pmr = (float)(p - r);
+                const V2 B2 = v2((float)b2d), Q = v2((float)q);
+                const V2 PF = v2((float)p), NPF = v2(-(float)p), RF = v2((float)r);
+                const V2 RMP = v2((float)(r - p)), NRMP = v2(-(float)(r - p)), PMR = v2((float)(p - r));
                 // RZ node G^5 (p cos (2p^2 + 2r^2 - zl^2 - p r cos) - 3 p^2 r) rewritten as
                 // -p (cos G^3 + 3 G^5 (p - r cos)(r - p cos)) (G^5 D = G^3, D the squared
                 // distance): its cos G^3 sum is the RPhi sum, so only the second sum is
                 // accumulated, and the two are combined in FP64 after the loop
                 Acc4 a0, a1;
-                forNodes<LANES>(np, lane, a0, a1, [&](int k, Acc4 &acc) {
-                    const PhiNode32 nd = pn[k];
-                    const float wc = 0.5f * nd.w * (nd.omcm - nd.omc);
-                    const float den = fmaf(b2, nd.omc, qf), denm = fmaf(b2, nd.omcm, qf);
-                    const float gq = rsqrtNR(den), gqm = rsqrtNR(denm);
-                    const float g3 = gq * gq * gq, g5 = g3 * gq * gq;
-                    const float g3m = gqm * gqm * gqm, g5m = g3m * gqm * gqm;
-                    const float rpc = fmaf(pf, nd.omc, rmp), prc = fmaf(rf, nd.omc, pmr);
-                    const float rpcm = fmaf(pf, nd.omcm, rmp), prcm = fmaf(rf, nd.omcm, pmr);
-                    acc.a = fmaf(wc, g3 - g3m, acc.a);
-                    acc.b = fmaf(wc, fmaf(g5, rpc, -g5m * rpcm), acc.b);
-                    acc.d = fmaf(nd.w, fmaf(g5, prc, g5m * prcm), acc.d);
-                    acc.c = fmaf(nd.w, fmaf(g5 * prc, rpc, g5m * prcm * rpcm), acc.c);
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc4 &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                    const V2 gq = rsq2(fma2(B2, nd.omc, Q)), gqm = rsq2(fma2(B2, nd.omcm, Q));
+                    const V2 g3 = gq * gq * gq, g5 = g3 * gq * gq;
+                    const V2 g3m = gqm * gqm * gqm, g5m = g3m * gqm * gqm;
+                    const V2 rpc = fma2(PF, nd.omc, RMP), prc = fma2(RF, nd.omc, PMR);
+                    const V2 rpcm = fma2(PF, nd.omcm, RMP), prcm = fma2(RF, nd.omcm, PMR);
+                    acc.a = fma2(wc, g3 - g3m, acc.a);
+                    acc.b = fma2(wc, fma2(g5, rpc, g5m * fma2(NPF, nd.omcm, NRMP)), acc.b);
+                    acc.d = fma2(nd.w, fma2(g5, prc, g5m * prcm), acc.d);
+                    acc.c = fma2(nd.w, fma2(g5 * prc, rpc, g5m * prcm * rpcm), acc.c);
                 });
-                const double w = l.y * t.y, ca = (double)a0.a + (double)a1.a;
+                const double w = l.y * t.y, ca = hsum(a0.a) + hsum(a1.a);
                 rphi += w * p * zl / r * ca;
-                rr += -3.0 * w * p * zl * ((double)a0.b + (double)a1.b);
-                zz += -3.0 * w * p * zl * ((double)a0.d + (double)a1.d);
-                rz += -w * p * (ca + 3.0 * ((double)a0.c + (double)a1.c));
+                rr += -3.0 * w * p * zl * (hsum(a0.b) + hsum(a1.b));
+                zz += -3.0 * w * p * zl * (hsum(a0.d) + hsum(a1.d));
+                rz += -w * p * (ca + 3.0 * (hsum(a0.c) + hsum(a1.c)));
             }
         }
     }

@@ -287,12 +287,11 @@ __device__ __forceinline__ void transformDerivatives(double yA, double zA, doubl
 #ifndef CCOIL_PAIR_MIN_BLOCKS
 #define CCOIL_PAIR_MIN_BLOCKS 6
 #endif
-// the same for the FP32 variants (M and F/T): 9 (56 registers) measured best
-// on B200 against 6, 7, 8 and 10 (M 70.3 ms at 2^18 arrangements against
-// 78.3, 73.7, 71.8 and 73.1; F/T flat at 48 ms); the FP32 kernel's lanes wait
-// on fixed-latency chains, which more resident warps hide
+// the same for the FP32 variants (M and F/T), whose packed integrands hold two
+// mirror pairs per value: 6 measured best against 4 and 5 (M 75.8, 87.2 and
+// 80.0 ms at 2^18 arrangements; F/T 75.9, 79.3, 75.7 ms)
 #ifndef CCOIL_PAIR32_MIN_BLOCKS
-#define CCOIL_PAIR32_MIN_BLOCKS 9
+#define CCOIL_PAIR32_MIN_BLOCKS 6
 #endif
 // largest single-primary blob staged in shared memory (0 turns staging off)
 #ifndef CCOIL_PAIR_STAGE_MAX_BYTES
@@ -335,16 +334,16 @@ __device__ __noinline__ double2 pairB64(const SegmentHeader &h, const double2 *t
 // over the secondary's nodes averages their rounding (measured: the same error
 // statistics against FP64 as with compensated sums, at 7-18 % less time)
 __device__ __noinline__ double pairA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                       const PhiNode32 *pn, const Frame &f)
+                                       const PhiPair2 *pn, const Frame &f)
 {
     return segmentA32<1, PlainSum, false>(h, tt, lt, pn, f, 0);
 }
 
 __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                        const PhiNode32 *pn, const Frame &f)
+                                        const PhiPair2 *pn, const Frame &f)
 {
     double H, Z;
-    segmentB32<1, PlainSum>(h, tt, lt, pn, f, 0, H, Z);
+    segmentB32<1, PlainSum, false>(h, tt, lt, pn, f, 0, H, Z);
     return make_double2(H, Z);
 }
 
@@ -406,8 +405,8 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
             const double2 *st = reinterpret_cast<const double2 *>(base) + ph.off_st;
             const SecAngular *sa = reinterpret_cast<const SecAngular *>(reinterpret_cast<const double2 *>(base) +
                                                                         ph.off_sa);
-            const PhiNode32 *pn = reinterpret_cast<const PhiNode32 *>(reinterpret_cast<const double2 *>(base) +
-                                                                      h.off_f32);
+            const PhiPair2 *pn = reinterpret_cast<const PhiPair2 *>(reinterpret_cast<const double2 *>(base) +
+                                                                    h.off_f32);
             __syncwarp();  // every lane is done with the previous pose
             if (lane == 0)
             {
@@ -822,11 +821,13 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     ph.off_sl = h.off_phi + h.n_phi;
     ph.off_st = ph.off_sl + ph.s_nl;
     ph.off_sa = ph.off_st + ph.s_nt;
-    std::vector<PhiNode32> p32;
+    std::vector<PhiPair2> p32;
     if (fp32)
     {
-        // FP32 angular mirror-pair table (16-byte entries) after the secondary tables
-        buildPhiPairs32(pp, p32);
+        // FP32 angular mirror-pair table (32-byte entries of two pairs) after the secondary tables
+        std::vector<PhiNode32> single;
+        buildPhiPairs32(pp, single);
+        packPhiPairs2(single.data(), (int)single.size(), p32);
         h.off_f32 = ph.off_sa + 2 * ph.s_na;
         setNearBox(prim, h);
     }
@@ -852,7 +853,7 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
             lengthUnits(pp, lu_);
         lengthUnits(spa, slu_);
         thicknessUnits(spa, stu_);
-        const int base16 = ph.off_sa + 2 * ph.s_na + (int)p32.size();
+        const int base16 = ph.off_sa + 2 * ph.s_na + 2 * (int)p32.size();
         ph.off_tu = base16;
         ph.off_lu = ph.off_tu + (int)tu_.size() / 2;
         ph.off_slu = ph.off_lu + (int)lu_.size() / 2;
@@ -871,7 +872,7 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     put(blob, sl_.data(), sizeof(double) * sl_.size());
     put(blob, st_.data(), sizeof(double) * st_.size());
     put(blob, sa_.data(), sizeof(SecAngular) * sa_.size());
-    put(blob, p32.data(), sizeof(PhiNode32) * p32.size());
+    put(blob, p32.data(), sizeof(PhiPair2) * p32.size());
     put(blob, tu_.data(), sizeof(double) * tu_.size());
     put(blob, lu_.data(), sizeof(double) * lu_.size());
     put(blob, slu_.data(), sizeof(double) * slu_.size());

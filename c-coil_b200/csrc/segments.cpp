@@ -81,6 +81,20 @@ PhiNode32 phiPair32(const PrecisionArgs &p, int k)
     return e;
 }
 
+void packPhiPairs2(const PhiNode32 *pairs, int count, std::vector<PhiPair2> &out)
+{
+    out.resize((size_t)(count + 1) / 2);
+    for (int m = 0; 2 * m < count; ++m)
+    {
+        const PhiNode32 &a = pairs[2 * m];
+        const PhiNode32 &b = 2 * m + 1 < count ? pairs[2 * m + 1] : PhiNode32{0.0f, a.omc, a.omcm, 0.0f};
+        out[m].omc = make_float2(a.omc, b.omc);
+        out[m].omcm = make_float2(a.omcm, b.omcm);
+        out[m].w = make_float2(a.w, b.w);
+        out[m].w2c2 = make_float2(a.w2c2, b.w2c2);
+    }
+}
+
 void buildPhiPairs32(const PrecisionArgs &p, std::vector<PhiNode32> &pairs)
 {
     const int n = p.angular_blocks * p.angular_increments;
@@ -174,9 +188,10 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
 
         const int headerBytes = (int)sizeof(SegmentHeader);
         const int fixedBytes = headerBytes + 16 * (int)(tNodes.size() + lNodes.size());
-        // FP32 mode: 16 bytes per FP64 node plus 16 per pair entry, and segments
-        // cut at even node counts so that no mirror pair is split
-        const int maxPhi = fp32 ? 2 * ((kSegmentBytes - fixedBytes) / 48) : (kSegmentBytes - fixedBytes) / 16;
+        // FP32 mode: 16 bytes per FP64 node plus 32 per two mirror pairs, and
+        // segments cut at multiples of four nodes so that no pair, and no packed
+        // entry of two pairs, is split
+        const int maxPhi = fp32 ? 4 * ((kSegmentBytes - fixedBytes) / 96) : (kSegmentBytes - fixedBytes) / 16;
         if (maxPhi < 1)
         {
             err = "coil " + std::to_string(ci) + ": thickness/length node tables exceed one staging segment";
@@ -212,7 +227,11 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
                       out.append(lNodes.data(), 16 * lNodes.size()) &&
                       out.append(phiNodes.data() + start, 16 * (size_t)cnt);
             if (ok && fp32)
-                ok = out.append(phi32.data() + start / 2, 16 * (size_t)((cnt + 1) / 2));
+            {
+                std::vector<PhiPair2> packed;
+                packPhiPairs2(phi32.data() + start / 2, (cnt + 1) / 2, packed);
+                ok = out.append(packed.data(), sizeof(PhiPair2) * packed.size());
+            }
             d.bytes = (int)((long long)out.size() - d.offset);
             if (!ok || !out.segment(d))
             {
