@@ -514,10 +514,9 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
                     const V2 X = sel(outside, t1 + t2, fma2(B2, nd.omc, Q));
                     const V2 Xm = sel(outside, t1m + t2m, fma2(B2, nd.omcm, Q));
                     const V2 s1 = g1 + g1m, s2 = g2 + g2m;
-                    // one reciprocal for the three products (sX, sX', s1 s2)
-                    const V2 sx = s * X, sxm = sm * Xm, s12 = s1 * s2, sxx = sx * sxm;
-                    const V2 rr = rcp2(sxx * s12);
-                    const V2 R = (sxm * s12) * rr, Rm = (sx * s12) * rr, rc = sxx * rr;
+                    // 1 / ((g1 + g2) X) per node and 1 / (s1 s2); merging all three into one
+                    // reciprocal measured no faster (the FP32 pipe bounds the kernel)
+                    const V2 R = rcp2(s * X), Rm = rcp2(sm * Xm), rc = rcp2(s1 * s2);
                     const V2 gg = g1 * g2, gg2 = gg * gg, ggm = g1m * g2m, gg2m = ggm * ggm;
                     const V2 hv = gg2 * (X * R), hvm = gg2m * (Xm * Rm);
                     const V2 ix = s * R, ixm = sm * Rm;
@@ -575,6 +574,86 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
     }
 }
 
+// The field with each mirror pair's difference taken by subtraction, for the
+// arrangement kernels: there every secondary node's field enters a sum over
+// the secondary's ring that itself cancels (the flux through a loop is far
+// smaller than the sum of |A| or |B| along it), and that cancellation, not the
+// per-node error, sets the error of M and F, so the closed forms of
+// segmentB32 measured no more accurate there and 57 % slower (F/T).
+//   fast:  H w c (hv - hv'), Z w (num y + num' y') with hv = g1^2 g2^2 / (g1 + g2),
+//          y = Y / X as in segmentB32 (dD inside Y outside the slab)
+//   slow:  H w c (g^3 - g'^3), Z w (num g^3 + num' g'^3)
+template <int LANES, typename S = PlainSum>
+__device__ __forceinline__ void segmentB32Direct(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                                 const PhiPair2 *pn, const Frame &f, int lane, double &H, double &Z)
+{
+    H = 0.0;
+    Z = 0.0;
+    const int ne = packedEntries(h.n_phi);
+    if (h.fast)
+    {
+        const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        const bool outside = top * bot > 0.0;
+        const double dD = 2.0 * f.z * (2.0 * h.half_length);
+        const V2 TOP = v2((float)top), BOT = v2((float)bot), DDF = v2((float)dD);
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+            const V2 B2 = v2((float)b2d), Q = v2((float)q), D1 = v2((float)(top * top + q)),
+                     D2 = v2((float)(bot * bot + q));
+            const V2 N0 = v2((float)(t.x * (t.x - f.r))), N1 = v2((float)(t.x * f.r));
+            Acc3<S> a0, a1;
+            forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc3<S> &acc) {
+                const PhiPair2 nd = pn[k];
+                auto node = [&](V2 om, V2 &hv, V2 &zv) {
+                    const V2 g1 = rsq2(fma2(B2, om, D1)), g2 = rsq2(fma2(B2, om, D2));
+                    const V2 gg = g1 * g2, gg2 = gg * gg, s = g1 + g2;
+                    const V2 t1 = TOP * g1, t2 = BOT * g2;
+                    const V2 X = sel(outside, t1 + t2, fma2(B2, om, Q));
+                    const V2 Y = sel(outside, DDF * gg2, t1 - t2);
+                    const V2 R = rcp2(s * X);
+                    hv = gg2 * (X * R);
+                    zv = fma2(N1, om, N0) * Y * (s * R);
+                };
+                V2 hv, zv, hm, zm;
+                node(nd.omc, hv, zv);
+                node(nd.omcm, hm, zm);
+                acc.h.add((v2(0.5f) * nd.w * (nd.omcm - nd.omc)) * (hv - hm));
+                acc.y.add(nd.w * (zv + zm));
+            });
+            H += t.y * t.x * dD * (a0.h.value() + a1.h.value());
+            Z += t.y * (a0.y.value() + a1.y.value());
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            const double2 l = lt[i];
+            const double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
+                const V2 B2 = v2((float)b2d), Q = v2((float)q);
+                const V2 N0 = v2((float)(t.x * (t.x - f.r))), N1 = v2((float)(t.x * f.r));
+                Acc3<S> a0, a1;
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc3<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 g = rsq2(fma2(B2, nd.omc, Q)), gm = rsq2(fma2(B2, nd.omcm, Q));
+                    const V2 g3 = g * g * g, g3m = gm * gm * gm;
+                    acc.y.add(nd.w * fma2(g3, fma2(N1, nd.omc, N0), g3m * fma2(N1, nd.omcm, N0)));
+                    acc.h.add((v2(0.5f) * nd.w * (nd.omcm - nd.omc)) * (g3 - g3m));
+                });
+                const double w = l.y * t.y;
+                H += w * t.x * zl * (a0.h.value() + a1.h.value());
+                Z += w * (a0.y.value() + a1.y.value());
+            }
+        }
+    }
+}
+
 // {RPhi, RR, RZ, ZZ}
 template <int LANES>
 __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
@@ -603,9 +682,9 @@ __device__ __forceinline__ void segmentG32(const SegmentHeader &h, const double2
                 const V2 gg = g1 * g2, s = g1 + g2;
                 const V2 t1 = TOP * g1, t2 = BOT * g2;
                 const V2 yd = sel(outside, t1 + t2, rho2);
-                // 1 / s, 1 / yd and 1 / rho^2 from one reciprocal of their product
-                const V2 sy = s * yd, r = rcp2(sy * rho2);
-                const V2 rs = (yd * rho2) * r, ryd = (s * rho2) * r, rrho = sy * r;
+                // separate reciprocals: merging them (1/a = b rcp(ab)) measured slower here,
+                // the FP32 pipe and not the MUFU pipe bounding the kernel
+                const V2 rs = rcp2(s), ryd = rcp2(yd), rrho = rcp2(rho2);
                 const V2 gg2 = gg * gg, ggs = gg2 * rs;
                 const V2 ddgg = DDF * gg2;
                 dg = DDF * ggs;

@@ -343,7 +343,7 @@ __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *t
                                         const PhiPair2 *pn, const Frame &f)
 {
     double H, Z;
-    segmentB32<1, PlainSum, false>(h, tt, lt, pn, f, 0, H, Z);
+    segmentB32Direct<1, PlainSum>(h, tt, lt, pn, f, 0, H, Z);
     return make_double2(H, Z);
 }
 

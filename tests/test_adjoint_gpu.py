@@ -234,10 +234,12 @@ def test_position_gradient_against_reference_force_1024_pairs(ccoil, reference):
 
     The two are different quadratures of the same integral (the force integrates
     t x B over the secondary's nodes; the gradient differentiates the A quadrature),
-    so at PF 5 they agree up to the quadrature error.  Where the secondary's winding
-    passes within 1 cm of the primary's, the integrand is nearly singular and both
-    quadratures are far from converged at PF 5 (and at PF 9); those pairs are
-    reported, not judged.  Everywhere else they agree to 1e-6."""
+    so at PF 5 they agree up to the quadrature error, which grows as the secondary's
+    winding nears the primary's (the integrand nears a singularity).  The test
+    asserts the median agreement (1e-7), agreement within 1e-6 for every pair whose
+    windings stay at least 5 cm apart, and that the discrepancy shrinks with the
+    PrecisionFactor (at PF 9 the median falls 100-fold and the 95th percentile
+    10-fold), i.e. that it is quadrature error."""
     from ccoil_b200 import workloads
     prim_row, sec_row, ppos, spos, py, pz, sy, sz = workloads.pair_config(arrangements=1024, seed=77,
                                                                           coaxial_fraction=0.0)
@@ -249,11 +251,14 @@ def test_position_gradient_against_reference_force_1024_pairs(ccoil, reference):
     args = (prim, sec, ppos, spos, py, pz, sy, sz)
     f_ref = reference.ft_arrangements(prim_row, sec_row, ppos, spos, py, pz, sy, sz, pf=5.0, method=0)[:, :3] / 6.0
     g5 = ccoil.Coil.compute_all_mutual_inductance_gradient_arrangements(*args, ccoil.PrecisionFactor(5.0))
+    g9 = ccoil.Coil.compute_all_mutual_inductance_gradient_arrangements(*args, ccoil.PrecisionFactor(9.0))
     f5 = ccoil.Coil.compute_all_force_torque_arrangements(*args, ccoil.PrecisionFactor(5.0))[:, :3] / 6.0
+    f9 = ccoil.Coil.compute_all_force_torque_arrangements(*args, ccoil.PrecisionFactor(9.0))[:, :3] / 6.0
     norm = np.linalg.norm
     # this library's FP64 force at PF 5 is the reference's to rounding
     assert np.max(norm(f5 - f_ref, axis=1) / norm(f_ref, axis=1)) < 1e-10
     e5 = norm(g5 - f_ref, axis=1) / norm(f_ref, axis=1)
+    e9 = norm(g9 - f9, axis=1) / norm(f9, axis=1)
     # distance from the secondary's winding (sampled: 24 angles x 9 lengths) to the
     # primary's winding cross-section [R, R + a] x [-b/2, b/2] in the primary's frame
     R1, a1, b1 = prim_row[:3]
@@ -262,15 +267,20 @@ def test_position_gradient_against_reference_force_1024_pairs(ccoil, reference):
     lz = np.linspace(-b2 / 2, b2 / 2, 9)
     ring = np.stack(np.broadcast_arrays(R2 * np.cos(phi)[:, None], R2 * np.sin(phi)[:, None], lz[None, :]),
                     -1).reshape(-1, 3)
-    near = np.zeros(len(sy), bool)
+    dist = np.zeros(len(sy))
     for i in range(len(sy)):
         A = _frame(sy[i], sz[i])  # the secondary's axes; the primary sits at the origin, unrotated
         q = ring @ A.T + spos[i]
         r, z = np.hypot(q[:, 0], q[:, 1]), q[:, 2]
         dr = np.maximum(np.maximum(R1 - r, r - (R1 + a1)), 0.0)
         dz = np.maximum(np.abs(z) - b1 / 2, 0.0)
-        near[i] = np.min(np.hypot(dr, dz)) < 0.01
-    print("|g - F| / |F| at PF 5: median %.2e; %d pairs clear of the winding: max %.2e; %d near it: max %.2e" % (
-        np.median(e5), (~near).sum(), e5[~near].max(), near.sum(), e5[near].max(initial=0.0)))
-    assert (~near).sum() >= 800
-    assert e5[~near].max() < 1e-6, np.flatnonzero(~near & (e5 >= 1e-6))
+        dist[i] = np.min(np.hypot(dr, dz))
+    for lo, hi in ((0.0, 0.01), (0.01, 0.03), (0.03, 0.05), (0.05, 1.0)):
+        m = (dist >= lo) & (dist < hi)
+        print("windings %.2f-%.2f m apart: %4d pairs, |g - F| / |F| at PF 5 median %.1e max %.1e; PF 9 max %.1e"
+              % (lo, hi, m.sum(), np.median(e5[m]) if m.any() else 0, e5[m].max(initial=0), e9[m].max(initial=0)))
+    clear = dist >= 0.05
+    assert np.median(e5) < 1e-7
+    assert clear.sum() >= 500 and e5[clear].max() < 1e-6, np.flatnonzero(clear & (e5 >= 1e-6))
+    assert np.median(e9) < 0.01 * np.median(e5)
+    assert np.quantile(e9, 0.95) < 0.1 * np.quantile(e5, 0.95)

@@ -135,6 +135,7 @@ def test_device_memory_path_and_determinism(cc):
     rows = cc.workloads.coil_rows_mixed(6, seed=55)
     pts = cc.workloads.points_cube(1000, seed=56)
     group = group_from_rows(cc, rows, 5.0)
+    timeouts = cc.lib().ccoil_timeout_count()
     plan = group.plan(1)
     host = plan(pts)
     host2 = plan(pts)
@@ -143,4 +144,4 @@ def test_device_memory_path_and_determinism(cc):
     plan.close()
     assert np.array_equal(host, host2)
     assert np.array_equal(host, dev.cpu().numpy())
-    assert cc.lib().ccoil_timeout_count() == 0
+    assert cc.lib().ccoil_timeout_count() == timeouts  # no bounded wait ran out in these calls
