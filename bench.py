@@ -639,10 +639,6 @@ def main():
     else:
         bound, unit = "fp32-pipe", "TFLOP/s"
         achieved, peak = flops_launch / t_dom / 1e12, 2.0 * rates[4] / 1e12
-        ins, mufu = opcount.fp32_ops_per_point(fidx, coils)
-        ins, mufu = ins * a.points, mufu * a.points
-        model.update({"fp32_instructions_per_launch": ins, "mufu_ops_per_launch": mufu,
-                      "fp32_issue_frac": ins / t_dom / rates[4], "mufu_frac": mufu / t_dom / rates[5]})
     clk = r["clocks"] or {}
     if clk.get("sm_mhz"):
         # nominal B200 per-SM rates at the sampled clock: FP64 64 and FP32 128 FMA per clock,
@@ -651,7 +647,8 @@ def main():
         model["nominal_at_sampled_clock"] = {"fp64_fma_tflops": 2 * 148 * 64 * f / 1e12,
                                              "fp32_fma_tflops": 2 * 148 * 128 * f / 1e12,
                                              "mufu_tops": 148 * 16 * f / 1e12, "sm_mhz": clk["sm_mhz"]}
-    traffic = read_traffic(dom, headline_mode)
+    prof = read_profile(dom, headline_mode)
+    traffic = prof.get("traffic") if prof else None
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": r["step_ms"], "higher_is_better": True, "scaling": "weak",
@@ -675,6 +672,7 @@ def main():
                          "peak_source": "measured on this GPU by ccoil_measure_op_rates (FMA = 2 flops); "
                                         "achieved counts the reference's operations, one flop each",
                          "model": model,
+                         "ncu": prof,
                          "rates_measured": None if rates is None else {
                              "fp64_fma_tflops": 2 * rates[0] / 1e12, "fp32_fma_tflops": 2 * rates[4] / 1e12,
                              "mufu_tops": rates[5] / 1e12, "ddiv_gops": rates[1] / 1e9,
@@ -757,9 +755,10 @@ def ctypes_rates(cc):
     return list(v)
 
 
-def read_traffic(field, mode):
-    """DRAM bytes per launch of the field kernel from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def read_profile(field, mode):
+    """The committed ncu figures of the field kernel (DRAM traffic per 2^20-point
+    launch, pipe utilisation), or None."""
+    path = os.path.join(ROOT, "profiles", "kernels.json")
     try:
         with open(path) as f:
             d = json.load(f)

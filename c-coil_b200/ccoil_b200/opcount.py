@@ -15,13 +15,10 @@ Add, subtract and multiply each take one FP64-pipe instruction slot; a divide,
 square root or logarithm takes rate(FMA) / rate(op) slots, with the rates
 measured on the device by ccoil_measure_op_rates.
 
-FP32-compensated kernel.  Per node, the FP32 instructions (FMA pipe and ALU,
-including the four of each Kahan update of the vector potential and field
-sums) and the MUFU operations (reciprocal square root, reciprocal) of the
-kernel's own integrands, counted from integrands32.cuh; the kernel is bound
-by instruction issue (one FP32
-instruction per lane and cycle, the FP32 FMA peak) or by MUFU, whichever is
-slower for the mix.
+The FP32-compensated kernels do more arithmetic per node than the reference's
+integrand (closed-form mirror differences, compensated sums); their roofline
+counts the same algorithmic flops, and ncu's pipe utilisation (committed under
+profiles/) describes the kernels themselves.
 """
 
 # field index: 0 = A (E), 1 = B, 3 = G; (field, fast method) ->
@@ -30,14 +27,6 @@ OPS_PER_NODE_64 = {
     (0, True): (13, 2, 3, 1), (0, False): (5, 1, 1, 0),
     (1, True): (17, 3, 2, 0), (1, False): (11, 1, 1, 0),
     (3, True): (53, 6, 2, 0), (3, False): (33, 2, 1, 0),
-}
-# (field, fast) -> (FP32 FMA-pipe + ALU instructions, MUFU operations) per node:
-# the kernel evaluates mirror pairs of nodes, so these are half the count of
-# one pair step (both nodes' integrands and the pair's accumulation)
-OPS_PER_NODE_32 = {
-    (0, True): (24.5, 3), (0, False): (4, 1),
-    (1, True): (26, 3), (1, False): (10.5, 1),
-    (3, True): (39.5, 5), (3, False): (13.5, 1),
 }
 # algorithmic flops per node: every operation of the reference integrand counts one
 FLOPS_PER_NODE = {k: sum(v) for k, v in OPS_PER_NODE_64.items()}
@@ -93,23 +82,11 @@ def fp64_slots_per_point(field, coils, rates):
     return total
 
 
-def fp32_ops_per_point(field, coils):
-    """(FP32 instructions, MUFU operations) per point for the group in the FP32 kernel."""
-    f = _field(field)
-    ins = mufu = 0.0
-    for p, fast in _coils(coils):
-        nphi, ntl = nodes_of(p, fast)
-        i, m = OPS_PER_NODE_32[(f, fast)]
-        ins += nphi * ntl * i
-        mufu += nphi * ntl * m
-    return ins, mufu
-
-
 def summary(coils):
     return {"coils": len(coils), "nodes_per_point": group_nodes_per_point(coils),
             "flops_per_point": {k: group_flops_per_point(f, coils) for k, f in (("A", 0), ("B", 1), ("G", 3))}}
 
 
-__all__ = ["OPS_PER_NODE_64", "OPS_PER_NODE_32", "FLOPS_PER_NODE", "PER_T_FLOPS", "PER_POINT_FLOPS",
+__all__ = ["OPS_PER_NODE_64", "FLOPS_PER_NODE", "PER_T_FLOPS", "PER_POINT_FLOPS",
            "nodes_of", "coil_point_flops", "group_flops_per_point", "group_nodes_per_point",
-           "fp64_slots_per_point", "fp32_ops_per_point", "summary"]
+           "fp64_slots_per_point", "summary"]

@@ -574,6 +574,77 @@ __device__ __forceinline__ void segmentB32(const SegmentHeader &h, const double2
     }
 }
 
+// The vector potential with each mirror pair's difference taken by
+// subtraction (asinh(u) - asinh(u'), g - g'), for the arrangement kernels, for
+// the reason given at segmentB32Direct.
+template <int LANES, typename S = PlainSum>
+__device__ __forceinline__ double segmentA32Direct(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                                   const PhiPair2 *pn, const Frame &f, int lane)
+{
+    double sum = 0.0;
+    const int ne = packedEntries(h.n_phi);
+    if (h.fast)
+    {
+        const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        const bool outside = top * bot > 0.0;
+        const float topf = (float)top, botf = (float)bot;
+        const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
+        const V2 TOP = v2(topf), BOT = v2(botf), NBOT = v2(-botf), DDF = v2(dDf);
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            const double q = (t.x - f.r) * (t.x - f.r), b2d = 2.0 * t.x * f.r;
+            const float qf = (float)q, b2 = (float)b2d;
+            const float d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+            float u0;
+            {
+                const float e1 = d1 * rsqrtNR(d1), e2 = d2 * rsqrtNR(d2);
+                u0 = outside ? fabsf(dDf * rcpApprox(fmaf(topf, e2, botf * e1)))
+                             : fabsf(fmaf(topf, e2, -botf * e1) * rcpApprox(qf));
+            }
+            const unsigned mask = __activemask();
+            const int tier = __all_sync(mask, u0 < 0.25f) ? 0 : (__all_sync(mask, u0 <= 1.0f) ? 1 : 2);
+            const V2 B2 = v2(b2), D1 = v2(d1), D2 = v2(d2), Q = v2(qf);
+            Acc1<S> a0, a1;
+            forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc1<S> &acc) {
+                const PhiPair2 nd = pn[k];
+                auto arg = [&](V2 om) {
+                    const V2 den1 = fma2(B2, om, D1), den2 = fma2(B2, om, D2);
+                    const V2 s1 = den1 * rsq2(den1), s2 = den2 * rsq2(den2);
+                    const V2 num = sel(outside, DDF, fma2(TOP, s2, NBOT * s1));
+                    const V2 den = sel(outside, fma2(TOP, s2, BOT * s1), fma2(B2, om, Q));
+                    return num * rcp2(den);
+                };
+                const V2 diff = asinhTier2(arg(nd.omc), tier) - asinhTier2(arg(nd.omcm), tier);
+                acc.v.add((v2(0.5f) * nd.w * (nd.omcm - nd.omc)) * diff);
+            });
+            sum += t.y * t.x * (a0.v.value() + a1.v.value());
+        }
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            const double2 l = lt[i];
+            const double zl = l.x + f.z;
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double q = (t.x - f.r) * (t.x - f.r) + zl * zl, b2d = 2.0 * t.x * f.r;
+                const V2 B2 = v2((float)b2d), Q = v2((float)q);
+                Acc1<S> a0, a1;
+                forEntries<LANES>(ne, lane, a0, a1, [&](int k, Acc1<S> &acc) {
+                    const PhiPair2 nd = pn[k];
+                    const V2 g = rsq2(fma2(B2, nd.omc, Q)), gm = rsq2(fma2(B2, nd.omcm, Q));
+                    acc.v.add((v2(0.5f) * nd.w * (nd.omcm - nd.omc)) * (g - gm));
+                });
+                sum += l.y * t.y * t.x * (a0.v.value() + a1.v.value());
+            }
+        }
+    }
+    return sum;
+}
+
 // The field with each mirror pair's difference taken by subtraction, for the
 // arrangement kernels: there every secondary node's field enters a sum over
 // the secondary's ring that itself cancels (the flux through a loop is far

@@ -336,7 +336,7 @@ __device__ __noinline__ double2 pairB64(const SegmentHeader &h, const double2 *t
 __device__ __noinline__ double pairA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                        const PhiPair2 *pn, const Frame &f)
 {
-    return segmentA32<1, PlainSum, false>(h, tt, lt, pn, f, 0);
+    return segmentA32Direct<1, PlainSum>(h, tt, lt, pn, f, 0);
 }
 
 __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
