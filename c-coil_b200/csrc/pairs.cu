@@ -287,11 +287,12 @@ __device__ __forceinline__ void transformDerivatives(double yA, double zA, doubl
 #ifndef CCOIL_PAIR_MIN_BLOCKS
 #define CCOIL_PAIR_MIN_BLOCKS 6
 #endif
-// the same for the FP32 variants (M and F/T), whose packed integrands hold two
-// mirror pairs per value: 6 measured best against 4 and 5 (M 75.8, 87.2 and
-// 80.0 ms at 2^18 arrangements; F/T 75.9, 79.3, 75.7 ms)
+// the same for the FP32 variants (M and F/T, packed integrands with the
+// subtracted mirror differences): 9 measured best against 6 (M 69.6 and
+// 75.2 ms at 2^18 arrangements; F/T 48.0 and 48.5 ms); their lanes wait on
+// fixed-latency chains, which more resident warps hide
 #ifndef CCOIL_PAIR32_MIN_BLOCKS
-#define CCOIL_PAIR32_MIN_BLOCKS 6
+#define CCOIL_PAIR32_MIN_BLOCKS 9
 #endif
 // largest single-primary blob staged in shared memory (0 turns staging off)
 #ifndef CCOIL_PAIR_STAGE_MAX_BYTES
