@@ -15,8 +15,9 @@ float32 points; backward: the FP64 adjoint in both cases.
 
 differentiates the mutual inductance of n arrangements of one primary and one
 secondary with respect to both coils' R, a, b, N and every arrangement's
-poses, through the pair kernel's exact parameter gradient (FP64; node counts
-fixed at the given geometry).
+poses, through the pair kernel's exact parameter gradient (node counts fixed
+at the given geometry; FP64 for float64 poses, the primary's quadrature in
+FP32 for float32 poses).
 
 `mutual_inductance_position_gradient` is the exact derivative of the mutual
 inductance quadrature with respect to the secondary's position (the pair
@@ -145,8 +146,10 @@ class _MutualInductance(torch.autograd.Function):
             raise ValueError("poses must be (n, 5) arrays of equal shape")
         pp, sp = precisions
         s1, s2 = _pair_structs(g1, g2, pp, sp)
+        # float32 poses: the primary's quadrature in FP32 (FP64 near its winding and in the sums)
+        mode = PrecisionMode.FP32_COMPENSATED if poses2.dtype == torch.float32 else PrecisionMode.FP64
         out, _ = _pair_arrangements([s1], s2, [sp.to_struct()], p1, p2,
-                                    _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT)
+                                    _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, precision_mode=mode)
         out = out * (g1[3] * g2[3])
         ctx.out = out
         ctx.turns = (g1[3], g2[3])

@@ -269,6 +269,132 @@ __device__ __noinline__ void segmentAParams64(const SegmentHeader &h, const doub
     out[4] = dB;
 }
 
+// The same five derivatives with the primary's quadrature in FP32 (mirror
+// pairs, two per packed step, differences by subtraction as in the FP32
+// arrangement integrands; the FP64 sum over the secondary's nodes follows).
+// Per node h(c) multiplies c, so a pair adds w c (h(c) - h(-c)):
+//   fast  h_z = g1 - g2 = -dD g1^2 g2^2 / (g1 + g2),  h_r = -(r - p c) y,
+//         h_p = V - p (p - r c) y,  h_b = (g1 + g2) / 2,
+//         y = (top g1 - bot g2) / rho^2 (its cancellation-free form outside the slab),
+//         V = asinh(u) in the single-asinh form of segmentA32Direct
+//   slow  h_z = -zl g^3,  h_r = -(r - p c) g^3,  h_p = g - p (p - r c) g^3
+__device__ __noinline__ void segmentAParams32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                              const PhiPair2 *pn, const double2 *tu, const double2 *lu,
+                                              const Frame &f, double a, double *out)
+{
+    const double r = f.r;
+    const int ne = packedEntries(h.n_phi);
+    double Ar = 0.0, Az = 0.0, dR = 0.0, dA = 0.0, dB = 0.0;
+    const V2 RF = v2((float)r);
+    if (h.fast)
+    {
+        const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        const bool outside = top * bot > 0.0;
+        const float topf = (float)top, botf = (float)bot;
+        const float dDf = (float)(2.0 * f.z * (2.0 * h.half_length));
+        const V2 TOP = v2(topf), BOT = v2(botf), NBOT = v2(-botf), DDF = v2(dDf), NDDF = v2(-dDf);
+        for (int j = 0; j < h.n_t; ++j)
+        {
+            const double2 t = tt[j];
+            const double p = t.x, q = (p - r) * (p - r), b2d = 2.0 * p * r;
+            const float qf = (float)q, d1 = (float)(top * top + q), d2 = (float)(bot * bot + q);
+            float u0;
+            {
+                const float e1 = d1 * rsqrtNR(d1), e2 = d2 * rsqrtNR(d2);
+                u0 = outside ? fabsf(dDf * rcpApprox(fmaf(topf, e2, botf * e1)))
+                             : fabsf(fmaf(topf, e2, -botf * e1) * rcpApprox(qf));
+            }
+            const unsigned mask = __activemask();
+            const int tier = __all_sync(mask, u0 < 0.25f) ? 0 : (__all_sync(mask, u0 <= 1.0f) ? 1 : 2);
+            const V2 B2 = v2((float)b2d), Q = v2(qf), D1 = v2(d1), D2 = v2(d2), PF = v2((float)p);
+            const V2 RMP = v2((float)(r - p)), PMR = v2((float)(p - r));
+            Acc4 a0, a1;
+            forEntries<1>(ne, 0, a0, a1, [&](int k, Acc4 &acc) {
+                const PhiPair2 nd = pn[k];
+                auto node = [&](V2 om, V2 &hz, V2 &hr, V2 &hp, V2 &hb) {
+                    const V2 den1 = fma2(B2, om, D1), den2 = fma2(B2, om, D2), rho2 = fma2(B2, om, Q);
+                    const V2 g1 = rsq2(den1), g2 = rsq2(den2);
+                    const V2 s = g1 + g2, gg = g1 * g2, gg2 = gg * gg;
+                    const V2 t1 = TOP * g1, t2 = BOT * g2;
+                    const V2 X = sel(outside, t1 + t2, rho2);
+                    const V2 R = rcp2(s * X);
+                    const V2 y = sel(outside, DDF * gg2, t1 - t2) * (s * R);
+                    const V2 s1 = den1 * g1, s2 = den2 * g2;
+                    const V2 u = sel(outside, DDF, fma2(TOP, s2, NBOT * s1)) *
+                                 rcp2(sel(outside, fma2(TOP, s2, BOT * s1), rho2));
+                    const V2 V = asinhTier2(u, tier);
+                    hz = NDDF * gg2 * (X * R);
+                    hr = v2(0.0f) - fma2(PF, om, RMP) * y;
+                    hp = V - PF * fma2(RF, om, PMR) * y;
+                    hb = v2(0.5f) * s;
+                };
+                V2 hz, hr, hp, hb, hzm, hrm, hpm, hbm;
+                node(nd.omc, hz, hr, hp, hb);
+                node(nd.omcm, hzm, hrm, hpm, hbm);
+                const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                acc.a = fma2(wc, hz - hzm, acc.a);
+                acc.b = fma2(wc, hr - hrm, acc.b);
+                acc.c = fma2(wc, hp - hpm, acc.c);
+                acc.d = fma2(wc, hb - hbm, acc.d);
+            });
+            const double sz = hsum(a0.a) + hsum(a1.a), sr = hsum(a0.b) + hsum(a1.b);
+            const double sp = hsum(a0.c) + hsum(a1.c), sb = hsum(a0.d) + hsum(a1.d);
+            Ar += t.y * p * sr;
+            Az += t.y * p * sz;
+            dR += t.y * sp;
+            dA += t.y * tu[j].x * sp;
+            dB += t.y * p * sb;
+        }
+        dB -= a / (2.0 * h.half_length);
+    }
+    else
+    {
+        for (int i = 0; i < h.n_l; ++i)
+        {
+            const double2 l = lt[i];
+            const double zl = l.x + f.z;
+            const V2 NZL = v2(-(float)zl);
+            for (int j = 0; j < h.n_t; ++j)
+            {
+                const double2 t = tt[j];
+                const double p = t.x, q = (p - r) * (p - r) + zl * zl, b2d = 2.0 * p * r;
+                const V2 B2 = v2((float)b2d), Q = v2((float)q), PF = v2((float)p);
+                const V2 RMP = v2((float)(r - p)), PMR = v2((float)(p - r));
+                Acc4 a0, a1;
+                forEntries<1>(ne, 0, a0, a1, [&](int k, Acc4 &acc) {
+                    const PhiPair2 nd = pn[k];
+                    auto node = [&](V2 om, V2 &hz, V2 &hr, V2 &hp) {
+                        const V2 g = rsq2(fma2(B2, om, Q)), g3 = g * g * g;
+                        hz = NZL * g3;
+                        hr = v2(0.0f) - fma2(PF, om, RMP) * g3;
+                        hp = g - PF * fma2(RF, om, PMR) * g3;
+                    };
+                    V2 hz, hr, hp, hzm, hrm, hpm;
+                    node(nd.omc, hz, hr, hp);
+                    node(nd.omcm, hzm, hrm, hpm);
+                    const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                    acc.a = fma2(wc, hz - hzm, acc.a);
+                    acc.b = fma2(wc, hr - hrm, acc.b);
+                    acc.c = fma2(wc, hp - hpm, acc.c);
+                });
+                const double sz = hsum(a0.a) + hsum(a1.a), sr = hsum(a0.b) + hsum(a1.b);
+                const double sp = hsum(a0.c) + hsum(a1.c);
+                const double w = l.y * t.y;
+                Ar += w * p * sr;
+                Az += w * p * sz;
+                dR += w * sp;
+                dA += w * tu[j].x * sp;
+                dB += w * lu[i].x * p * sz;
+            }
+        }
+    }
+    out[0] = Ar;
+    out[1] = Az;
+    out[2] = dR;
+    out[3] = dA;
+    out[4] = dB;
+}
+
 // d T / d(y axis angle) and d T / d(z axis angle) of poseFromAngles' transform
 __device__ __forceinline__ void transformDerivatives(double yA, double zA, double *dTy, double *dTz)
 {
@@ -539,9 +665,17 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     const double2 *lu = reinterpret_cast<const double2 *>(base) + ph.off_lu;
                     const double ul = (reinterpret_cast<const double2 *>(base) + ph.off_slu)[l].x;
                     const double ut = (reinterpret_cast<const double2 *>(base) + ph.off_stu)[t].x;
-                    const double av = pairA64(h, tt, lt, pt, f);
-                    double d[5];
-                    segmentAParams64(h, tt, lt, pt, tu, lu, f, av, d);
+                    double av, d[5];
+                    if (FP32 && far)
+                    {
+                        av = pairA32(h, tt, lt, pn, f);
+                        segmentAParams32(h, tt, lt, pn, tu, lu, f, av, d);
+                    }
+                    else
+                    {
+                        av = pairA64(h, tt, lt, pt, f);
+                        segmentAParams64(h, tt, lt, pt, tu, lu, f, av, d);
+                    }
                     const double ar = d[0], az = d[1];
                     const double c = f.cphi, s_ = f.sphi;
                     const double ao = f.r > 0.0 ? av / f.r : ar;
@@ -928,9 +1062,9 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
                            "the parameter gradient needs exactly one primary with per-arrangement poses");
     if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown precision mode");
-    if (precision == CCOIL_PRECISION_FP32_COMPENSATED && (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT ||
-                                                          quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT))
-        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "the mutual-inductance gradients are evaluated in FP64 only");
+    if (precision == CCOIL_PRECISION_FP32_COMPENSATED && quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED,
+                           "the position gradient is evaluated in FP64 only (the parameter gradient has an FP32 form)");
     const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
     if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
@@ -1050,8 +1184,10 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
         CCOIL_PAIR_LAUNCH(1, true);
     else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
         CCOIL_PAIR_LAUNCH(2, false);
-    else
+    else if (!fp32)
         CCOIL_PAIR_LAUNCH(3, false);
+    else
+        CCOIL_PAIR_LAUNCH(3, true);
 #undef CCOIL_PAIR_LAUNCH
     if (zPass && cudaGetLastError() == cudaSuccess)
     {

@@ -198,7 +198,7 @@ typedef enum ccoil_pair_quantity
                                                            R inner radius, a thickness, b length).  The primary's
                                                            position gradient is -dM/d(x2, y2, z2) and
                                                            dM/dN = M / N for either coil.  One primary with
-                                                           per-arrangement poses; FP64 only. */
+                                                           per-arrangement poses; FP64 or FP32_COMPENSATED. */
 } ccoil_pair_quantity_t;
 
 /* Position and orientation of a coil (Coil::setPositionAndOrientation,
@@ -233,8 +233,9 @@ typedef struct ccoil_pose
  * uses the reference's z-axis formulas); their number is returned in
  * *z_axis_count.
  * precision: CCOIL_PRECISION_FP64 follows the reference's double arithmetic;
- * CCOIL_PRECISION_FP32_COMPENSATED (mutual inductance and force/torque only;
- * CCOIL_ERR_NOT_SUPPORTED for the gradient) evaluates the primary's quadrature
+ * CCOIL_PRECISION_FP32_COMPENSATED (mutual inductance, force/torque and the
+ * parameter gradient; CCOIL_ERR_NOT_SUPPORTED for the position gradient)
+ * evaluates the primary's quadrature
  * in FP32 with compensated sums, except where a secondary node lies within the
  * primary's near-field box (winding cross-section inflated by 0.1 R), which
  * is evaluated in FP64; sums over secondary nodes and primaries are FP64. */

@@ -287,3 +287,48 @@ def test_position_gradient_against_reference_force_1024_pairs(ccoil, reference):
     apart = dist >= 0.01  # the windings do not cross
     assert np.median(e9[apart]) < 0.01 * np.median(e5[apart])
     assert np.quantile(e9[apart], 0.95) < 0.1 * np.quantile(e5[apart], 0.95)
+
+
+def test_mutual_inductance_parameter_gradient_fp32(ccoil):
+    """Pair quantity 3 with the primary's quadrature in FP32 (FP32_COMPENSATED; FP64
+    near the winding and in every sum) against FP64: M and its 13 derivatives on 2,048
+    arrangements of the arrangement workload, each column within 1e-5 of its largest
+    FP64 magnitude (the FP32 path's M is within 1.2e-5 of FP64 at its worst
+    arrangement, relative to 1e-3 of the batch's largest M); the float32 torch
+    Function takes that path and keeps its gradients within the same bar."""
+    import torch
+    from ccoil_b200 import workloads
+    from ccoil_b200.autograd import mutual_inductance, pair_precisions_for
+    prim_row, sec_row, ppos, spos, py, pz, sy, sz = workloads.pair_config(arrangements=2048, seed=57,
+                                                                          coaxial_fraction=0.05)
+    prim, sec = workloads.coils_from_rows(prim_row, 5.0)[0], workloads.coils_from_rows(sec_row, 5.0)[0]
+    args = (prim, sec, ppos, spos, py, pz, sy, sz, ccoil.PrecisionFactor(5.0))
+    from ccoil_b200 import _lib
+    from ccoil_b200.coil import _pair_arrangements
+    pp, sp = ccoil.Coil._pair_args(prim, sec, 5.0)
+    p1 = np.concatenate([ppos, py[:, None], pz[:, None]], axis=1)
+    p2 = np.concatenate([spos, sy[:, None], sz[:, None]], axis=1)
+    res = []
+    for mode in (ccoil.PrecisionMode.FP64, ccoil.PrecisionMode.FP32_COMPENSATED):
+        out, _ = _pair_arrangements([prim.struct(pp)], sec.struct(sp), [sp.to_struct()], p1, p2,
+                                    _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, precision_mode=mode)
+        res.append(out)
+    d64, d32 = res
+    err = np.max(np.abs(d32 - d64), axis=0) / np.max(np.abs(d64), axis=0)
+    print("FP32 parameter gradient, max error per column relative to its largest value:",
+          " ".join("%.1e" % e for e in err))
+    assert err.max() < 1e-5, err
+    # the float32 torch Function
+    g1 = np.array([0.1, 0.05, 0.1, 200.0])
+    g2 = np.array([0.05, 0.0, 0.2, 100.0])
+    precs = pair_precisions_for(g1, g2, 5.0)
+    grads = []
+    for dt in (torch.float64, torch.float32):
+        G1 = torch.tensor(g1, dtype=dt, requires_grad=True)
+        G2 = torch.tensor(g2, dtype=dt, requires_grad=True)
+        P1 = torch.tensor(p1[:256], dtype=dt, requires_grad=True)
+        P2 = torch.tensor(p2[:256], dtype=dt, requires_grad=True)
+        mutual_inductance(G1, G2, P1, P2, precs).sum().backward()
+        grads.append([x.grad.double().numpy() for x in (G1, G2, P1, P2)])
+    for a, b in zip(*grads):
+        assert np.max(np.abs(b - a)) <= 1e-5 * np.max(np.abs(a)), (np.max(np.abs(b - a)), np.max(np.abs(a)))
