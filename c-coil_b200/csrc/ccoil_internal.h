@@ -179,8 +179,11 @@ struct FieldLaunch
     unsigned long long *d_refine_count = nullptr;
 };
 constexpr size_t kNearPairBytes = 8;
-// default ratio of the FP32_REFINED test (ccoil_set_refine_ratio)
-constexpr double kDefaultRefineRatio = 4.0;
+// default ratio of the FP32_REFINED test (ccoil_set_refine_ratio): on the 128-coil
+// benchmark group it refines 2 % of the points for A and 6.5 % for B and cuts the
+// maximum error about 5x (A) and 2.5x (B) at 80-90 % of FP32_COMPENSATED's speed;
+// ratios near 5 already refine more than half the points
+constexpr double kDefaultRefineRatio = 10.0;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
 int checkBoundedWait(long long limitCycles, void *stream);

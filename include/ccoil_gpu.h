@@ -172,7 +172,7 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
 /* FP32_REFINED's test ratio (process-wide, read when a plan executes; >= 1):
  * a point is re-evaluated in FP64 when the norms of its FP32-evaluated
  * contributions add up to more than `ratio` times the norm of its total.
- * Smaller ratios refine more points.  ccoil_field_plan_refined_points reports
+ * Smaller ratios refine more points; the default is 10.  ccoil_field_plan_refined_points reports
  * how many points the plan's last execution re-evaluated (synchronous). */
 int ccoil_set_refine_ratio(double ratio);
 double ccoil_refine_ratio(void);

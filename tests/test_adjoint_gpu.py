@@ -292,8 +292,8 @@ def test_position_gradient_against_reference_force_1024_pairs(ccoil, reference):
 def test_mutual_inductance_parameter_gradient_fp32(ccoil):
     """Pair quantity 3 with the primary's quadrature in FP32 (FP32_COMPENSATED; FP64
     near the winding and in every sum) against FP64: M and its 13 derivatives on 2,048
-    arrangements of the arrangement workload, each column within 1e-5 of its largest
-    FP64 magnitude (the FP32 path's M is within 1.2e-5 of FP64 at its worst
+    arrangements of the arrangement workload, each column (or group of columns of one
+    scale) within 1e-5 of its largest FP64 magnitude (the FP32 path's M is within 1.2e-5 of FP64 at its worst
     arrangement, relative to 1e-3 of the batch's largest M); the float32 torch
     Function takes that path and keeps its gradients within the same bar."""
     import torch
@@ -314,8 +314,11 @@ def test_mutual_inductance_parameter_gradient_fp32(ccoil):
                                     _lib.PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT, precision_mode=mode)
         res.append(out)
     d64, d32 = res
-    err = np.max(np.abs(d32 - d64), axis=0) / np.max(np.abs(d64), axis=0)
-    print("FP32 parameter gradient, max error per column relative to its largest value:",
+    # columns in groups that share a scale: M; each geometry parameter; both angles of a
+    # coil (the primary sits at y angle 0 here, where dM/dz angle vanishes); the position
+    groups = [[0], [1], [2], [3], [4, 5], [6], [7], [8], [9, 10, 11], [12, 13]]
+    err = np.array([np.max(np.abs(d32[:, g] - d64[:, g])) / np.max(np.abs(d64[:, g])) for g in groups])
+    print("FP32 parameter gradient, max error per column group relative to its largest value:",
           " ".join("%.1e" % e for e in err))
     assert err.max() < 1e-5, err
     # the float32 torch Function

@@ -1,10 +1,14 @@
 """FP32-compensated field path against the FP64 path (which reproduces the
 reference's double CPU results to 1e-12, see test_fields_gpu.py).
 
-Error is the norm-wise relative error per point.  The bars below are what the
-path guarantees on these workloads (median < 3e-7, 99th percentile < 2e-6,
-max < 1e-5); the residual error comes from the azimuthal cancellation of far
-points and from cancellation between coils of opposite current.  Near-field (point, coil) pairs
+Error is the norm-wise relative error per point.  One coil at a time, the
+closed-form mirror differences keep the error flat with distance
+(test_single_coil_far_field: max below 1e-6 out to 40 coil radii, where
+subtracting the mirror nodes lost up to 2e-5).  A group adds the cancellation
+between coils of opposite current, which multiplies the per-coil error by
+sum |F_c| / |sum F_c| (up to ~100 on the benchmark workload).  The 16-coil
+group workload measures median 2.4-5.0e-8, 99th percentile 1.1-1.8e-7 and
+max 4.1-6.0e-7 for A, B and E; its bars sit 2-3x above that.  Near-field (point, coil) pairs
 are evaluated with the FP64 integrands and must match the FP64 path exactly up
 to summation order; the gradient is compared outside its ill-conditioned band,
 where the FP64 reference form itself carries ~1e-7 rounding noise."""
@@ -38,9 +42,10 @@ def test_group_workload_error(ccoil, field):
     e = rel_err(f32, f64)
     if field == 3:
         e = e[~gradient_band(rows, pts)]
-    assert np.median(e) < 3e-7, np.median(e)
-    assert np.quantile(e, 0.99) < 2e-6, np.quantile(e, 0.99)
-    assert e.max() < 1e-5, e.max()
+    print(field, "median %.1e p99 %.1e max %.1e" % (np.median(e), np.quantile(e, 0.99), e.max()))
+    assert np.median(e) < 1e-7, np.median(e)
+    assert np.quantile(e, 0.99) < 4e-7, np.quantile(e, 0.99)
+    assert e.max() < 2e-6, e.max()
 
 
 def test_single_rect_workload_error(ccoil):
@@ -53,6 +58,29 @@ def test_single_rect_workload_error(ccoil):
         if field == 3:
             e = e[~gradient_band(rows, pts)]
         assert np.median(e) < 3e-7 and e.max() < 1e-5, (field, np.median(e), e.max())
+
+
+@pytest.mark.parametrize("row", [[0.1, 0.05, 0.08, 100, 1.0, 50.0, 0, 0, 0, 0.4, 1.0],   # RECTANGULAR
+                                 [0.1, 0.0, 0.08, 100, 1.0, 50.0, 0, 0, 0, 0.4, 1.0],    # THIN
+                                 [0.1, 0.05, 0.0, 100, 1.0, 50.0, 0, 0, 0, 0.4, 1.0],    # FLAT
+                                 [0.1, 0.0, 0.0, 100, 1.0, 50.0, 0, 0, 0, 0.4, 1.0]])    # FILAMENT
+def test_single_coil_far_field(ccoil, row):
+    """One coil, points at 1.5 to 40 coil radii in random directions: A and B within
+    1e-6 of FP64 at every point (the far-field azimuthal cancellation is removed by
+    the closed-form mirror differences), median below 1e-7."""
+    from ccoil_b200 import workloads
+    g = np.random.default_rng(13)
+    n = 8192
+    d = 0.1 * np.exp(g.uniform(np.log(1.5), np.log(40.0), n))
+    v = g.normal(size=(n, 3))
+    pts = v / np.linalg.norm(v, axis=1, keepdims=True) * d[:, None]
+    rows = np.array([row], dtype=float)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    for field in (0, 1):
+        f64, f32 = (evaluate(ccoil, coils, pts, field, m) for m in modes(ccoil))
+        e = rel_err(f32, f64)
+        print(row[:3], field, "median %.1e p99 %.1e max %.1e" % (np.median(e), np.quantile(e, 0.99), e.max()))
+        assert np.median(e) < 1e-7 and e.max() < 1e-6, (row[:3], field, np.median(e), e.max())
 
 
 def test_near_field_pairs_use_fp64(ccoil):
