@@ -86,6 +86,7 @@ def lib():
     L.ccoil_field_plan_destroy.argtypes = [vp]
     L.ccoil_timeout_count.restype = ctypes.c_longlong
     L.ccoil_check_bounded_wait.argtypes = [ctypes.c_longlong, vp]
+    L.ccoil_set_point_ordering.argtypes = [ctypes.c_int]
     L.ccoil_set_refine_ratio.argtypes = [ctypes.c_double]
     L.ccoil_refine_ratio.restype = ctypes.c_double
     L.ccoil_field_plan_refined_points.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]

@@ -71,6 +71,8 @@ std::atomic<int> g_failAllocations{0};
 std::atomic<double> g_refineRatio{kDefaultRefineRatio};
 // device-side wait timeouts already reported to a caller
 std::atomic<long long> g_timeoutsReported{0};
+// FP32 plans sort their points along a Morton curve (ccoil_set_point_ordering)
+std::atomic<int> g_pointOrdering{1};
 } // namespace
 
 cudaError_t scratchAlloc(void **p, size_t bytes, cudaStream_t st)
@@ -157,6 +159,7 @@ struct ccoil_field_plan
     SegmentSet set;
     DeviceBuffer blob, segs, points, out, work, workCount;
     DeviceBuffer cabs, refine, refineCount;  // FP32_REFINED
+    DeviceBuffer orderScratch, order, sortedPoints, sortedOut;  // point ordering
 };
 
 extern "C" {
@@ -348,7 +351,32 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
         L.refine_capacity = plan->refine.bytes / sizeof(int);
         L.d_refine_count = static_cast<unsigned long long *>(plan->refineCount.ptr);
     }
+    // FP32 modes: evaluate the points in Morton order (ordering.cu)
+    const bool ordered = g_pointOrdering.load() != 0 && plan->precision != CCOIL_PRECISION_FP64 &&
+                         point_count >= kPointOrderMinPoints && point_count <= kPointOrderMaxPoints;
+    if (ordered)
+    {
+        const size_t scratch = pointOrderScratchBytes(point_count);
+        int rc0 = plan->orderScratch.reserve(scratch);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->order.reserve(sizeof(int) * (size_t)point_count);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->sortedPoints.reserve(inBytes);
+        if (rc0 == CCOIL_OK)
+            rc0 = plan->sortedOut.reserve(outBytes);
+        if (rc0 == CCOIL_OK)
+            rc0 = orderPoints(dPoints, point_count, plan->orderScratch.ptr, plan->orderScratch.bytes,
+                              static_cast<int *>(plan->order.ptr), static_cast<double *>(plan->sortedPoints.ptr),
+                              stream);
+        if (rc0 != CCOIL_OK)
+            return rc0;
+        L.d_points = static_cast<const double *>(plan->sortedPoints.ptr);
+        L.d_out = static_cast<double *>(plan->sortedOut.ptr);
+    }
     int rc = launchFields(L, stream);
+    if (rc == CCOIL_OK && ordered)
+        rc = scatterResults(static_cast<const double *>(plan->sortedOut.ptr), static_cast<const int *>(plan->order.ptr),
+                            point_count, width, dOut, stream);
     if (rc != CCOIL_OK)
         return rc;
 
@@ -385,6 +413,10 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
     plan->cabs.release();
     plan->refine.release();
     plan->refineCount.release();
+    plan->orderScratch.release();
+    plan->order.release();
+    plan->sortedPoints.release();
+    plan->sortedOut.release();
     delete plan;
     return CCOIL_OK;
 }
@@ -424,6 +456,14 @@ int ccoil_check_bounded_wait(long long limit_cycles, void *stream)
         g_timeoutsReported.store(count);
     return rc;
 }
+
+int ccoil_set_point_ordering(int enabled)
+{
+    g_pointOrdering.store(enabled ? 1 : 0);
+    return CCOIL_OK;
+}
+
+int ccoil_point_ordering(void) { return g_pointOrdering.load(); }
 
 int ccoil_set_refine_ratio(double ratio)
 {

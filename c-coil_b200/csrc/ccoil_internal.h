@@ -186,6 +186,18 @@ constexpr size_t kNearPairBytes = 8;
 constexpr double kDefaultRefineRatio = 10.0;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
+
+// Point ordering of the FP32 field plans (ordering.cu): sort the points along
+// a Morton curve over their bounding box so that each warp's points lie close
+// together, evaluate them in that order, scatter the results back.
+// orderPoints writes the permutation (order[i] = caller's index of sorted
+// point i) and the sorted points; scratch holds pointOrderScratchBytes(n).
+constexpr long long kPointOrderMinPoints = 1LL << 14;
+constexpr long long kPointOrderMaxPoints = 1LL << 30;
+size_t pointOrderScratchBytes(long long n);
+int orderPoints(const double *pts, long long n, void *scratch, size_t scratchBytes, int *order, double *sortedPts,
+                void *stream);
+int scatterResults(const double *sorted, const int *order, long long n, int width, double *out, void *stream);
 int checkBoundedWait(long long limitCycles, void *stream);
 
 // batched persistent launch (fields.cu, batch.cuh)

@@ -440,37 +440,49 @@ struct WarpPose
 
 // FP64 primary quadrature at one secondary node, out of line for the FP32
 // kernel (which takes it only for near-field nodes) so that its register
-// budget does not carry the FP64 integrands
-__device__ __noinline__ double pairA64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                       const double2 *pt, const Frame &f)
+// budget does not carry the FP64 integrands.  The point's frame coordinates
+// pass by value (the quadrature reads z and r only), so nothing of the
+// caller's has to sit in memory for the call.
+__device__ __forceinline__ Frame frameZR(double z, double r)
 {
-    return segmentA64<1>(h, tt, lt, pt, f, 0);
+    Frame f;
+    f.z = z;
+    f.r = r;
+    f.cphi = 1.0;
+    f.sphi = 0.0;
+    return f;
+}
+
+__device__ __noinline__ double pairA64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                       const double2 *pt, double z, double r)
+{
+    return segmentA64<1>(h, tt, lt, pt, frameZR(z, r), 0);
 }
 
 __device__ __noinline__ double2 pairB64(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                        const double2 *pt, const Frame &f)
+                                        const double2 *pt, double z, double r)
 {
     double H, Z;
-    segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
+    segmentB64<1>(h, tt, lt, pt, frameZR(z, r), 0, H, Z);
     return make_double2(H, Z);
 }
 
-// The FP32 primary quadrature, out of line as well: the call saves the
-// secondary-node state once per node, and the loop over the primary's nodes
-// gets the whole register budget.  Its pair sums are plain FP32: the FP64 sum
-// over the secondary's nodes averages their rounding (measured: the same error
-// statistics against FP64 as with compensated sums, at 7-18 % less time)
+// The FP32 primary quadrature, out of line as well: the loop over the
+// primary's nodes gets the whole register budget.  Its pair sums are plain
+// FP32: the FP64 sum over the secondary's nodes averages their rounding
+// (measured: the same error statistics against FP64 as with compensated sums,
+// at 7-18 % less time)
 __device__ __noinline__ double pairA32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                       const PhiPair2 *pn, const Frame &f)
+                                       const PhiPair2 *pn, double z, double r)
 {
-    return segmentA32Direct<1, PlainSum>(h, tt, lt, pn, f, 0);
+    return segmentA32Direct<1, PlainSum>(h, tt, lt, pn, frameZR(z, r), 0);
 }
 
 __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                        const PhiPair2 *pn, const Frame &f)
+                                        const PhiPair2 *pn, double z, double r)
 {
     double H, Z;
-    segmentB32Direct<1, PlainSum>(h, tt, lt, pn, f, 0, H, Z);
+    segmentB32Direct<1, PlainSum>(h, tt, lt, pn, frameZR(z, r), 0, H, Z);
     return make_double2(H, Z);
 }
 
@@ -500,6 +512,14 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
     extern __shared__ __align__(16) unsigned char stagedPair[];
     __shared__ WarpPose warpPoses[4];
     __shared__ int nearLists[4][64];  // FP32: each warp's deferred near-field secondary nodes
+    constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : QTY == 2 ? 3 : 14;
+    // Running sums in shared memory: each thread's sums over its secondary nodes
+    // (one column per thread, so a warp's accesses hit 32 consecutive doubles)
+    // and each warp's sums over the primaries (lane 0).  Held in registers they
+    // stayed live across the out-of-line quadrature call and spilled to local
+    // memory at the register budget of 9 CTAs per SM.
+    __shared__ double laneSums[W][128];
+    __shared__ double warpSums[4][W];
     if (stagedBytes > 0)
     {
         const int4 *src = reinterpret_cast<const int4 *>(blob + primOffsets[0]);
@@ -508,17 +528,17 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
             dst[i] = src[i];
         __syncthreads();
     }
-    constexpr int W = QTY == 0 ? 1 : QTY == 1 ? 6 : QTY == 2 ? 3 : 14;
     const int lane = threadIdx.x % 32;
     volatile WarpPose &S = warpPoses[threadIdx.x / 32];
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const long long warps = (long long)gridDim.x * blockDim.x / 32;
+    double *part = &laneSums[0][threadIdx.x];  // part[128 i]: this thread's sum i
+    double *total = warpSums[threadIdx.x / 32];
     for (long long a = warp; a < count; a += warps)
     {
-        double total[W];
-#pragma unroll
-        for (int i = 0; i < W; ++i)
-            total[i] = 0.0;
+        if (lane == 0)
+            for (int i = 0; i < W; ++i)
+                total[i] = 0.0;
         bool hasZ = false;  // lane 0: some primary of this arrangement is left to the z-axis pass
         for (int j = 0; j < nprim; ++j)
         {
@@ -602,10 +622,8 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
             if (S.skip)
                 continue;  // warp-uniform: the z-axis pass adds this primary
             const int nsec = ph.s_nl * ph.s_nt * ph.s_na;
-            double part[W];
-#pragma unroll
             for (int i = 0; i < W; ++i)
-                part[i] = 0.0;
+                part[128 * i] = 0.0;
             // every lane runs the same number of iterations (warp-uniform choices
             // below); a lane past the end evaluates the last node and drops it
             // One secondary node per lane.  mode 0: the FP64 kernel; mode 1: the FP32
@@ -646,11 +664,11 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                 {
                     double av;
                     if (!FP32)
-                        av = CCOIL_PAIR_CALL_FP64 ? pairA64(h, tt, lt, pt, f) : segmentA64<1>(h, tt, lt, pt, f, 0);
+                        av = CCOIL_PAIR_CALL_FP64 ? pairA64(h, tt, lt, pt, f.z, f.r) : segmentA64<1>(h, tt, lt, pt, f, 0);
                     else if (far)
-                        av = pairA32(h, tt, lt, pn, f);
+                        av = pairA32(h, tt, lt, pn, f.z, f.r);
                     else
-                        av = pairA64(h, tt, lt, pt, f);
+                        av = pairA64(h, tt, lt, pt, f.z, f.r);
                     const double vx = -av * f.sphi, vy = av * f.cphi;
                     const double Ax = S.T[0] * vx + S.T[1] * vy, Ay = S.T[3] * vx + S.T[4] * vy,
                                  Az = S.T[6] * vx + S.T[7] * vy;
@@ -668,12 +686,12 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     double av, d[5];
                     if (FP32 && far)
                     {
-                        av = pairA32(h, tt, lt, pn, f);
+                        av = pairA32(h, tt, lt, pn, f.z, f.r);
                         segmentAParams32(h, tt, lt, pn, tu, lu, f, av, d);
                     }
                     else
                     {
-                        av = pairA64(h, tt, lt, pt, f);
+                        av = pairA64(h, tt, lt, pt, f.z, f.r);
                         segmentAParams64(h, tt, lt, pt, tu, lu, f, av, d);
                     }
                     const double ar = d[0], az = d[1];
@@ -742,7 +760,7 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     g[13] = gB;
                     if (valid)
                         for (int i = 0; i < 14; ++i)
-                            part[i] += g[i] * w;
+                            part[128 * i] += g[i] * w;
                 }
                 else if (QTY == 2)
                 {
@@ -765,7 +783,7 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         o[i] = S.T[3 * i] * v[0] + S.T[3 * i + 1] * v[1] + S.T[3 * i + 2] * v[2];
                     if (valid)
                         for (int i = 0; i < 3; ++i)
-                            part[i] += o[i] * w;
+                            part[128 * i] += o[i] * w;
                 }
                 else
                 {
@@ -774,7 +792,7 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
                     else
                     {
-                        const double2 hz = FP32 && far ? pairB32(h, tt, lt, pn, f) : pairB64(h, tt, lt, pt, f);
+                        const double2 hz = FP32 && far ? pairB32(h, tt, lt, pn, f.z, f.r) : pairB64(h, tt, lt, pt, f.z, f.r);
                         H = hz.x;
                         Z = hz.y;
                     }
@@ -790,8 +808,8 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     if (valid)
                         for (int i = 0; i < 3; ++i)
                         {
-                            part[i] += dF[i];
-                            part[3 + i] += dT[i];
+                            part[128 * i] += dF[i];
+                            part[128 * (3 + i)] += dT[i];
                         }
                 }
             };
@@ -821,15 +839,17 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         n0 += 32;
                     }
                 }
-#pragma unroll
-            for (int off = 16; off > 0; off /= 2)
-#pragma unroll
-                for (int i = 0; i < W; ++i)
-                    part[i] += __shfl_xor_sync(0xffffffffu, part[i], off);
             const double scale = QTY == 1 ? ph.f_factor : ph.m_factor;
 #pragma unroll
             for (int i = 0; i < W; ++i)
-                total[i] += part[i] * scale;
+            {
+                double v = part[128 * i];
+#pragma unroll
+                for (int off = 16; off > 0; off /= 2)
+                    v += __shfl_xor_sync(0xffffffffu, v, off);
+                if (lane == 0)
+                    total[i] += v * scale;
+            }
         }
         if (lane == 0)
         {

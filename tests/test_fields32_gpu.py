@@ -225,3 +225,43 @@ def test_refined_mode(ccoil):
     finally:
         L.ccoil_set_refine_ratio(ctypes.c_double(default))
     assert L.ccoil_set_refine_ratio(ctypes.c_double(0.5)) == 1
+
+
+def test_point_ordering(ccoil):
+    """FP32 plans of at least 16,384 points evaluate them in Morton order and scatter
+    the results back: every result lands at its caller's index (against FP64, which
+    keeps the caller's order, at the group bars), ordered and unordered evaluation
+    agree to FP32 rounding, the ordered results repeat exactly, and points with a
+    non-finite coordinate give non-finite results at their own index only.  Ordering
+    applies to FP32_REFINED too."""
+    import ctypes
+    from ccoil_b200 import workloads
+    L = ccoil.lib()
+    assert L.ccoil_point_ordering() == 1
+    rows = workloads.coil_rows_mixed(16, seed=77)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    pts = workloads.points_cube(40000, seed=31)
+    bad = [5, 17000, 39999]
+    pts[bad[0], 0] = np.nan
+    pts[bad[1], 2] = np.inf
+    pts[bad[2], 1] = -np.inf
+    good = np.ones(len(pts), dtype=bool)
+    good[bad] = False
+    try:
+        for field in (0, 1, 3):
+            f64 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP64)
+            on = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
+            again = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
+            refined = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_REFINED)
+            L.ccoil_set_point_ordering(0)
+            off = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
+            L.ccoil_set_point_ordering(1)
+            assert not np.isfinite(on[bad]).any() and not np.isfinite(off[bad]).any(), field
+            assert np.array_equal(on, again, equal_nan=True), field
+            keep = good if field != 3 else good & ~gradient_band(rows, pts)
+            for got in (on, refined):
+                e = rel_err(got[keep], f64[keep])
+                assert np.median(e) < 1e-7 and e.max() < 2e-6, (field, np.median(e), e.max())
+            assert rel_err(on[good], off[good]).max() < 2e-6, field
+    finally:
+        L.ccoil_set_point_ordering(1)
