@@ -63,30 +63,35 @@ struct SegmentDesc
 // Every squared distance the integrands use is Q + b2 (1 - cos), so the second
 // node's exceed the first's by the same delta = b2 (omcm - omc) = 2 b2 c.  The
 // FP32 integrands form f(c) - f(-c) as delta times a cancellation-free
-// expression and g(c) + g(-c) directly; the entry carries
-// w2c2 = w (omcm - omc)^2 / 2 = 2 w c^2, the weight of such a difference divided
-// by b2, computed from the FP32 values of omc and omcm so that it matches the
-// distances the kernels form from them.  With an odd node count the middle
-// node (c = 0) is an entry of its own with half its weight (evaluated twice,
-// w2c2 = 0).
+// expression and g(c) + g(-c) directly; the entry carries the weights of
+// such terms, computed in FP64 from the FP32 values of omc and omcm (so that
+// they match the distances the kernels form from them) and rounded once:
+// w2c2 = w (omcm - omc)^2 / 2 = 2 w c^2, the weight of a difference divided by
+// b2; wc = w (omcm - omc) / 2 = w c; ws2 = w omc omcm = w sin^2.  With an odd
+// node count the middle node (c = 0) is an entry of its own with half its
+// weight (evaluated twice, w2c2 = wc = 0).
 struct alignas(16) PhiNode32
 {
     float w2c2;  // w (omcm - omc)^2 / 2 (0 for the middle node)
     float omc;   // 1 - cos(phi_k) = 2 sin^2(phi_k / 2)
     float omcm;  // 1 - cos(phi_{n-1-k}) = 2 sin^2(phi_{n-1-k} / 2) (about 2 - omc)
     float w;     // w_phi (halved for the middle node)
+    float wc;    // w (omcm - omc) / 2
+    float ws2;   // w omc omcm
 };
 
 // Device layout of the FP32 angular table: two consecutive mirror pairs per
-// 32-byte entry, every field a float2 {pair 2m, pair 2m + 1}, so the integrands
+// 48-byte entry, every field a float2 {pair 2m, pair 2m + 1}, so the integrands
 // evaluate both pairs with packed FP32 (f32x2) instructions.  A table with an
 // odd pair count ends in an entry whose second pair has zero weights and the
-// first pair's nodes (its values stay finite and add nothing).
+// first pair's nodes (its values stay finite and add nothing).  The weights
+// wc and ws2 save the integrands 2-5 packed instructions per entry, for one
+// more 16-byte load.
 struct alignas(16) PhiPair2
 {
-    float2 omc, omcm, w, w2c2;
+    float2 omc, omcm, w, w2c2, wc, ws2;
 };
-static_assert(sizeof(PhiPair2) == 32, "FP32 angular entries are 32 bytes");
+static_assert(sizeof(PhiPair2) == 48, "FP32 angular entries are 48 bytes");
 void packPhiPairs2(const PhiNode32 *pairs, int count, std::vector<PhiPair2> &out);
 
 // Node order of the FP64 angular table in FP32 mode: position j holds node

@@ -331,7 +331,7 @@ __device__ __noinline__ void segmentAParams32(const SegmentHeader &h, const doub
                 V2 hz, hr, hp, hb, hzm, hrm, hpm, hbm;
                 node(nd.omc, hz, hr, hp, hb);
                 node(nd.omcm, hzm, hrm, hpm, hbm);
-                const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                const V2 wc = nd.wc;
                 acc.a = fma2(wc, hz - hzm, acc.a);
                 acc.b = fma2(wc, hr - hrm, acc.b);
                 acc.c = fma2(wc, hp - hpm, acc.c);
@@ -372,7 +372,7 @@ __device__ __noinline__ void segmentAParams32(const SegmentHeader &h, const doub
                     V2 hz, hr, hp, hzm, hrm, hpm;
                     node(nd.omc, hz, hr, hp);
                     node(nd.omcm, hzm, hrm, hpm);
-                    const V2 wc = v2(0.5f) * nd.w * (nd.omcm - nd.omc);
+                    const V2 wc = nd.wc;
                     acc.a = fma2(wc, hz - hzm, acc.a);
                     acc.b = fma2(wc, hr - hrm, acc.b);
                     acc.c = fma2(wc, hp - hpm, acc.c);
@@ -979,7 +979,7 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
     std::vector<PhiPair2> p32;
     if (fp32)
     {
-        // FP32 angular mirror-pair table (32-byte entries of two pairs) after the secondary tables
+        // FP32 angular mirror-pair table (entries of two pairs) after the secondary tables
         std::vector<PhiNode32> single;
         buildPhiPairs32(pp, single);
         packPhiPairs2(single.data(), (int)single.size(), p32);
@@ -1008,7 +1008,7 @@ bool buildPair(const Coil &prim, const Coil &sec, const PrecisionArgs &pp, const
             lengthUnits(pp, lu_);
         lengthUnits(spa, slu_);
         thicknessUnits(spa, stu_);
-        const int base16 = ph.off_sa + 2 * ph.s_na + 2 * (int)p32.size();
+        const int base16 = ph.off_sa + 2 * ph.s_na + (int)(sizeof(PhiPair2) / 16 * p32.size());
         ph.off_tu = base16;
         ph.off_lu = ph.off_tu + (int)tu_.size() / 2;
         ph.off_slu = ph.off_lu + (int)lu_.size() / 2;

@@ -69,6 +69,7 @@ PhiNode32 phiPair32(const PrecisionArgs &p, int k)
     {
         e.omcm = e.omc;
         e.w2c2 = 0.0f;
+        e.wc = 0.0f;
         e.w = (float)(0.5 * w);
     }
     else
@@ -76,8 +77,10 @@ PhiNode32 phiPair32(const PrecisionArgs &p, int k)
         e.omcm = (float)(2.0 * sm * sm);
         const double twoC = (double)e.omcm - (double)e.omc;
         e.w2c2 = (float)(0.5 * w * twoC * twoC);
+        e.wc = (float)(0.5 * w * twoC);
         e.w = (float)w;
     }
+    e.ws2 = (float)((double)e.w * (double)e.omc * (double)e.omcm);
     return e;
 }
 
@@ -87,11 +90,14 @@ void packPhiPairs2(const PhiNode32 *pairs, int count, std::vector<PhiPair2> &out
     for (int m = 0; 2 * m < count; ++m)
     {
         const PhiNode32 &a = pairs[2 * m];
-        const PhiNode32 &b = 2 * m + 1 < count ? pairs[2 * m + 1] : PhiNode32{0.0f, a.omc, a.omcm, 0.0f};
+        const PhiNode32 &b =
+            2 * m + 1 < count ? pairs[2 * m + 1] : PhiNode32{0.0f, a.omc, a.omcm, 0.0f, 0.0f, 0.0f};
         out[m].omc = make_float2(a.omc, b.omc);
         out[m].omcm = make_float2(a.omcm, b.omcm);
         out[m].w = make_float2(a.w, b.w);
         out[m].w2c2 = make_float2(a.w2c2, b.w2c2);
+        out[m].wc = make_float2(a.wc, b.wc);
+        out[m].ws2 = make_float2(a.ws2, b.ws2);
     }
 }
 
@@ -188,10 +194,11 @@ bool buildFieldSegments(const Coil *coils, int count, int field, int precision, 
 
         const int headerBytes = (int)sizeof(SegmentHeader);
         const int fixedBytes = headerBytes + 16 * (int)(tNodes.size() + lNodes.size());
-        // FP32 mode: 16 bytes per FP64 node plus 32 per two mirror pairs, and
+        // FP32 mode: 16 bytes per FP64 node plus 48 per two mirror pairs, and
         // segments cut at multiples of four nodes so that no pair, and no packed
         // entry of two pairs, is split
-        const int maxPhi = fp32 ? 4 * ((kSegmentBytes - fixedBytes) / 96) : (kSegmentBytes - fixedBytes) / 16;
+        const int maxPhi = fp32 ? 4 * ((kSegmentBytes - fixedBytes) / (64 + (int)sizeof(PhiPair2)))
+                                : (kSegmentBytes - fixedBytes) / 16;
         if (maxPhi < 1)
         {
             err = "coil " + std::to_string(ci) + ": thickness/length node tables exceed one staging segment";
