@@ -441,9 +441,9 @@ def bench_pf_sweep(a):
 
 def bench_refine_sweep(a):
     """Cost curve of FP32_REFINED on the group workload: per field and refinement
-    ratio, the fraction of points re-evaluated in FP64, the time of the whole
-    evaluation and its error against FP64 (away from windings), beside plain
-    FP32_COMPENSATED and FP64."""
+    fraction, the share of (point, coil segment) pairs re-evaluated in FP64, the
+    time of the whole evaluation and its error against FP64 (away from windings),
+    beside plain FP32_COMPENSATED and FP64."""
     import ctypes
     import torch
     import ccoil_b200 as cc
@@ -458,8 +458,8 @@ def bench_refine_sweep(a):
     near, band = (torch.from_numpy(m).to(dev) for m in winding_masks(rows, pts_host))
     flush = flush_l2(torch, dev)
     L = cc.lib()
-    default_ratio = L.ccoil_refine_ratio()
-    ratios = [1.25, 1.5, 2.0, 3.0, 5.0, 10.0]
+    default_fraction = L.ccoil_refine_fraction()
+    fractions = [0.5, 0.2, 0.1, 0.05, 0.02]
 
     def timed(plan, out):
         for _ in range(max(a.warmup, 1)):
@@ -487,20 +487,20 @@ def bench_refine_sweep(a):
             res[label] = {"ms": timed(plan, outs[label])}
             plan.close()
         res["fp32c"]["err"] = rel_err_stats(outs["fp32c"], outs["fp64"], away)
-        for r in ratios:
-            L.ccoil_set_refine_ratio(ctypes.c_double(r))
+        for fr in fractions:
+            L.ccoil_set_refine_fraction(ctypes.c_double(fr))
             plan = group.plan(f, cc.PrecisionMode.FP32_REFINED)
             out = torch.empty((a.points, w), dtype=torch.float64, device=dev)
             ms = timed(plan, out)
-            res["ratio_%g" % r] = {"ms": ms, "refined_fraction": plan.refined_points() / a.points,
-                                   "err": rel_err_stats(out, outs["fp64"], away),
-                                   "speedup_vs_fp64": res["fp64"]["ms"] / ms}
+            res["fraction_%g" % fr] = {"ms": ms, "refined_pairs_per_point": plan.refined_pairs() / a.points,
+                                       "err": rel_err_stats(out, outs["fp64"], away),
+                                       "speedup_vs_fp64": res["fp64"]["ms"] / ms}
             plan.close()
         res["fp32c"]["speedup_vs_fp64"] = res["fp64"]["ms"] / res["fp32c"]["ms"]
         curve[name] = res
-    L.ccoil_set_refine_ratio(ctypes.c_double(default_ratio))
-    print(json.dumps({"workload": "refine-sweep", "default_ratio": default_ratio, "config": workload_config(a, 1), "steps": a.steps,
-                      "l2": "flushed between timed evaluations", "curve": curve}))
+    L.ccoil_set_refine_fraction(ctypes.c_double(default_fraction))
+    print(json.dumps({"workload": "refine-sweep", "default_fraction": default_fraction, "config": workload_config(a, 1),
+                      "steps": a.steps, "coils": a.coils, "l2": "flushed between timed evaluations", "curve": curve}))
 
 
 def main():

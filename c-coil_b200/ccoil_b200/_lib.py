@@ -87,9 +87,9 @@ def lib():
     L.ccoil_timeout_count.restype = ctypes.c_longlong
     L.ccoil_check_bounded_wait.argtypes = [ctypes.c_longlong, vp]
     L.ccoil_set_point_ordering.argtypes = [ctypes.c_int]
-    L.ccoil_set_refine_ratio.argtypes = [ctypes.c_double]
-    L.ccoil_refine_ratio.restype = ctypes.c_double
-    L.ccoil_field_plan_refined_points.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.ccoil_set_refine_fraction.argtypes = [ctypes.c_double]
+    L.ccoil_refine_fraction.restype = ctypes.c_double
+    L.ccoil_field_plan_refined_pairs.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.ccoil_inject_allocation_failures.argtypes = [ctypes.c_int]
     L.ccoil_batch_plan_create.argtypes = [cp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]

@@ -178,10 +178,11 @@ class FieldPlan:
                                              ctypes.c_void_p(stream or 0)))
         return res
 
-    def refined_points(self):
-        """Points the last execution re-evaluated in FP64 (FP32_REFINED plans)."""
+    def refined_pairs(self):
+        """(point, coil segment) pairs the last execution re-evaluated in FP64
+        (FP32_REFINED plans)."""
         n = ctypes.c_longlong()
-        check(lib().ccoil_field_plan_refined_points(self._h, ctypes.byref(n)))
+        check(lib().ccoil_field_plan_refined_pairs(self._h, ctypes.byref(n)))
         return n.value
 
     def close(self):

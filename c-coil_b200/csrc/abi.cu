@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -66,9 +67,9 @@ constexpr int kMaxDevices = 64;
 cudaMemPool_t g_pools[kMaxDevices] = {};
 // allocations still to fail on purpose (ccoil_inject_allocation_failures)
 std::atomic<int> g_failAllocations{0};
-// FP32_REFINED: re-evaluate a point in FP64 when the norms of its FP32
-// contributions add up to more than this ratio times the norm of its total
-std::atomic<double> g_refineRatio{kDefaultRefineRatio};
+// FP32_REFINED: re-evaluate in FP64 every (point, segment) pair whose FP32
+// contribution's norm exceeds this fraction of the norm of the point's total
+std::atomic<double> g_refineFraction{kDefaultRefineFraction};
 // device-side wait timeouts already reported to a caller
 std::atomic<long long> g_timeoutsReported{0};
 // FP32 plans sort their points along a Morton curve (ccoil_set_point_ordering)
@@ -158,7 +159,7 @@ struct ccoil_field_plan
     int coil_count = 0;
     SegmentSet set;
     DeviceBuffer blob, segs, points, out, work, workCount;
-    DeviceBuffer cabs, refine, refineCount;  // FP32_REFINED
+    DeviceBuffer contrib, refineSegs, refinedTotal;  // FP32_REFINED
     DeviceBuffer orderScratch, order, sortedPoints, sortedOut;  // point ordering
 };
 
@@ -317,12 +318,30 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
     L.field = plan->field;
     L.precision = plan->precision;
     L.lanes = lanes_per_point ? lanes_per_point : autoLanes(point_count);
+    // FP32_REFINED runs in chunks of points whose stored contributions fit
+    // kRefineContribBytes and whose pairs fit a list of kRefineListPairs
+    const bool refined = plan->precision == CCOIL_PRECISION_FP32_REFINED && L.nseg > 0;
+    long long chunk = point_count;
+    if (refined)
+    {
+        const size_t perPoint = (size_t)L.nseg * (size_t)width * sizeof(double);
+        long long maxChunk = (long long)(kRefineContribBytes / perPoint);
+        const long long byList = (long long)(kRefineListPairs / (unsigned long long)L.nseg);
+        maxChunk = std::max(1LL, std::min(maxChunk, byList));
+        const long long chunks = (point_count + maxChunk - 1) / maxChunk;
+        chunk = (point_count + chunks - 1) / chunks;
+        if (L.lanes > 8)
+            L.lanes = 8;  // the refining kernel is compiled for 1 to 8 lanes per point
+    }
     if (plan->precision == CCOIL_PRECISION_FP32_COMPENSATED || plan->precision == CCOIL_PRECISION_FP32_REFINED)
     {
         // near-field work list: room for every (point, segment) pair up to 4 Mi
-        // entries (32 MiB); pairs beyond it are integrated in FP64 in place
-        unsigned long long want = (unsigned long long)point_count * (unsigned long long)L.nseg;
-        unsigned long long cap = want < (1ULL << 22) ? want : (1ULL << 22);
+        // entries (32 MiB; FP32_REFINED: every pair of a chunk, up to
+        // kRefineListPairs); near-field pairs beyond it are integrated in FP64 in
+        // place
+        unsigned long long want = (unsigned long long)chunk * (unsigned long long)L.nseg;
+        const unsigned long long limit = refined ? kRefineListPairs : (1ULL << 22);
+        unsigned long long cap = want < limit ? want : limit;
         if (cap == 0)
             cap = 1;
         int rc0 = plan->work.reserve(cap * kNearPairBytes);
@@ -335,21 +354,22 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
         L.d_work_count = static_cast<unsigned long long *>(plan->workCount.ptr);
         L.near_blocks = 148 * 8;
     }
-    if (plan->precision == CCOIL_PRECISION_FP32_REFINED)
+    if (refined)
     {
-        // every point can be listed: the list never overflows
-        int rc0 = plan->cabs.reserve(sizeof(double) * (size_t)point_count);
+        int rc0 = plan->contrib.reserve((size_t)chunk * (size_t)L.nseg * (size_t)width * sizeof(double));
         if (rc0 == CCOIL_OK)
-            rc0 = plan->refine.reserve(sizeof(int) * (size_t)point_count);
+            rc0 = plan->refineSegs.reserve(sizeof(unsigned long long) * (size_t)L.nseg);
         if (rc0 == CCOIL_OK)
-            rc0 = plan->refineCount.reserve(sizeof(unsigned long long));
+            rc0 = plan->refinedTotal.reserve(sizeof(unsigned long long));
         if (rc0 != CCOIL_OK)
             return rc0;
-        L.refine_ratio = g_refineRatio.load();
-        L.d_cabs = static_cast<double *>(plan->cabs.ptr);
-        L.d_refine = static_cast<int *>(plan->refine.ptr);
-        L.refine_capacity = plan->refine.bytes / sizeof(int);
-        L.d_refine_count = static_cast<unsigned long long *>(plan->refineCount.ptr);
+        cudaError_t e = cudaMemsetAsync(plan->refinedTotal.ptr, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess)
+            return cudaFail(e, "refinement count");
+        L.refine_fraction = g_refineFraction.load();
+        L.d_contrib = static_cast<double *>(plan->contrib.ptr);
+        L.d_refine_segs = static_cast<unsigned long long *>(plan->refineSegs.ptr);
+        L.d_refined_total = static_cast<unsigned long long *>(plan->refinedTotal.ptr);
     }
     // FP32 modes: evaluate the points in Morton order (ordering.cu)
     const bool ordered = g_pointOrdering.load() != 0 && plan->precision != CCOIL_PRECISION_FP64 &&
@@ -373,7 +393,15 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
         L.d_points = static_cast<const double *>(plan->sortedPoints.ptr);
         L.d_out = static_cast<double *>(plan->sortedOut.ptr);
     }
-    int rc = launchFields(L, stream);
+    int rc = CCOIL_OK;
+    for (long long off = 0; off < point_count && rc == CCOIL_OK; off += chunk)
+    {
+        FieldLaunch C = L;
+        C.d_points = L.d_points + 3 * off;
+        C.d_out = L.d_out + (long long)width * off;
+        C.npts = std::min(chunk, point_count - off);
+        rc = launchFields(C, stream);
+    }
     if (rc == CCOIL_OK && ordered)
         rc = scatterResults(static_cast<const double *>(plan->sortedOut.ptr), static_cast<const int *>(plan->order.ptr),
                             point_count, width, dOut, stream);
@@ -410,9 +438,9 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
     plan->out.release();
     plan->work.release();
     plan->workCount.release();
-    plan->cabs.release();
-    plan->refine.release();
-    plan->refineCount.release();
+    plan->contrib.release();
+    plan->refineSegs.release();
+    plan->refinedTotal.release();
     plan->orderScratch.release();
     plan->order.release();
     plan->sortedPoints.release();
@@ -465,25 +493,25 @@ int ccoil_set_point_ordering(int enabled)
 
 int ccoil_point_ordering(void) { return g_pointOrdering.load(); }
 
-int ccoil_set_refine_ratio(double ratio)
+int ccoil_set_refine_fraction(double fraction)
 {
-    if (!(ratio >= 1.0) || !std::isfinite(ratio))
-        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "the refinement ratio must be finite and >= 1");
-    g_refineRatio.store(ratio);
+    if (!(fraction >= 0.0) || !std::isfinite(fraction))
+        return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "the refinement fraction must be finite and >= 0");
+    g_refineFraction.store(fraction);
     return CCOIL_OK;
 }
 
-double ccoil_refine_ratio(void) { return g_refineRatio.load(); }
+double ccoil_refine_fraction(void) { return g_refineFraction.load(); }
 
-int ccoil_field_plan_refined_points(ccoil_field_plan_t *plan, long long *count)
+int ccoil_field_plan_refined_pairs(ccoil_field_plan_t *plan, long long *count)
 {
     if (!plan || !count)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "null plan or count");
     *count = 0;
-    if (plan->precision != CCOIL_PRECISION_FP32_REFINED || !plan->refineCount.ptr)
+    if (plan->precision != CCOIL_PRECISION_FP32_REFINED || !plan->refinedTotal.ptr)
         return CCOIL_OK;
     unsigned long long v = 0;
-    cudaError_t e = cudaMemcpy(&v, plan->refineCount.ptr, sizeof(v), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(&v, plan->refinedTotal.ptr, sizeof(v), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess)
         return cudaFail(e, "refinement count");
     *count = (long long)v;

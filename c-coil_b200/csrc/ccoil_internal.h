@@ -175,20 +175,26 @@ struct FieldLaunch
     unsigned long long work_capacity = 0;
     unsigned long long *d_work_count = nullptr;
     int near_blocks = 0;                    // grid of the near-field pass
-    // FP32_REFINED: points whose FP32 contributions' norms add up to more than
-    // refine_ratio times the norm of their total are re-evaluated in FP64
-    double refine_ratio = 0.0;              // 0: no refinement
-    double *d_cabs = nullptr;               // double[npts] (scratch)
-    int *d_refine = nullptr;                // int[refine_capacity] (scratch)
-    unsigned long long refine_capacity = 0;
-    unsigned long long *d_refine_count = nullptr;
+    // FP32_REFINED: every (point, segment) FP32 contribution whose norm exceeds
+    // refine_fraction times the norm of the point's total is replaced by its
+    // FP64 value; the FP32 pass stores the contributions in d_contrib
+    // (nseg x npts x W doubles, scratch), the selection lists the pairs in the
+    // work list (which then needs room for them) and counts them in
+    // d_refined_total (not reset between calls)
+    double refine_fraction = 0.0;
+    double *d_contrib = nullptr;
+    unsigned long long *d_refine_segs = nullptr;  // nseg counters (scratch)
+    unsigned long long *d_refined_total = nullptr;
 };
 constexpr size_t kNearPairBytes = 8;
-// default ratio of the FP32_REFINED test (ccoil_set_refine_ratio): on the 128-coil
-// benchmark group it refines 2 % of the points for A and 6.5 % for B and cuts the
-// maximum error about 5x (A) and 2.5x (B) at 80-90 % of FP32_COMPENSATED's speed;
-// ratios near 5 already refine more than half the points
-constexpr double kDefaultRefineRatio = 10.0;
+// default fraction of FP32_REFINED (ccoil_set_refine_fraction): on the 128-coil
+// benchmark group it re-evaluates about 12 % of the (point, coil) pairs in FP64
+// and brings the maximum relative error of A and B below 1e-7
+constexpr double kDefaultRefineFraction = 0.1;
+// FP32_REFINED evaluates the points in chunks whose stored contributions fit
+// this many bytes, and lists at most kRefineListPairs pairs per chunk
+constexpr size_t kRefineContribBytes = size_t(1) << 31;
+constexpr unsigned long long kRefineListPairs = 1ULL << 25;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
 

@@ -221,30 +221,38 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     if (blocks > 2147483647LL)
         return cudaErrorInvalidConfiguration;
     const bool fp32 = L.precision == CCOIL_PRECISION_FP32_COMPENSATED || L.precision == CCOIL_PRECISION_FP32_REFINED;
-    const bool refine = fp32 && L.refine_ratio > 0.0 && L.d_cabs && L.d_refine && L.d_refine_count;
-    double *cabs = refine ? L.d_cabs : nullptr;
+    const bool refine =
+        L.precision == CCOIL_PRECISION_FP32_REFINED && L.d_contrib && L.d_refine_segs && L.d_refined_total;
+    // the refining kernel is compiled for 1 to 8 lanes per point
+    if (refine && L.lanes > 8)
+        return cudaErrorInvalidValue;
     const bool staged = fp32 ? CCOIL_FP32_STAGE : CCOIL_FP64_STAGE;
     const size_t smem = staged ? (size_t)kSegmentStages * kSegmentBytes : 0;
     NearPair *work = reinterpret_cast<NearPair *>(L.d_work);
     switch (L.lanes)
     {
-#define CCOIL_CASE(N)                                                                                             \
+#define CCOIL_LAUNCH32(N, R)                                                                                      \
+    fieldsKernel32<FIELD, N, R><<<(unsigned)blocks, threads, smem, st>>>(                                         \
+        L.d_blob, L.d_segs, L.nseg, L.d_points, L.npts, L.d_out, work, L.work_capacity, L.d_work_count,           \
+        R ? L.d_contrib : nullptr)
+#define CCOIL_CASE(N, REFINING)                                                                                   \
     case N:                                                                                                       \
-        if (fp32)                                                                                                 \
-            fieldsKernel32<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(                                    \
-                L.d_blob, L.d_segs, L.nseg, L.d_points, L.npts, L.d_out, work, L.work_capacity, L.d_work_count,   \
-                cabs);                                                                                            \
+        if (refine)                                                                                               \
+            CCOIL_LAUNCH32(N, REFINING);                                                                          \
+        else if (fp32)                                                                                            \
+            CCOIL_LAUNCH32(N, false);                                                                             \
         else                                                                                                      \
             fieldsKernel64<FIELD, N><<<(unsigned)blocks, threads, smem, st>>>(L.d_blob, L.d_segs, L.nseg,         \
                                                                               L.d_points, L.npts, L.d_out);       \
         break;
-        CCOIL_CASE(1)
-        CCOIL_CASE(2)
-        CCOIL_CASE(4)
-        CCOIL_CASE(8)
-        CCOIL_CASE(16)
-        CCOIL_CASE(32)
+        CCOIL_CASE(1, true)
+        CCOIL_CASE(2, true)
+        CCOIL_CASE(4, true)
+        CCOIL_CASE(8, true)
+        CCOIL_CASE(16, false)
+        CCOIL_CASE(32, false)
 #undef CCOIL_CASE
+#undef CCOIL_LAUNCH32
         default: return cudaErrorInvalidValue;
     }
     cudaError_t e = cudaGetLastError();
@@ -257,12 +265,23 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     e = cudaGetLastError();
     if (e != cudaSuccess || !refine)
         return e;
+    // FP32_REFINED: with the near-field pairs in, select the dominating
+    // contributions into a segment-major list (the work list is reused), take
+    // them out of the totals and add them back in FP64
     constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
-    const long long testBlocks = std::min<long long>((L.npts + 255) / 256, 148LL * 16);
-    refineTestKernel<W><<<(unsigned)testBlocks, 256, 0, st>>>(L.d_out, L.d_cabs, L.npts, L.refine_ratio, L.d_refine,
-                                                             L.refine_capacity, L.d_refine_count);
-    refineKernel64<FIELD, 4><<<148 * 8, 128, 0, st>>>(L.d_blob, L.d_segs, L.nseg, L.d_points, L.d_out, L.d_refine,
-                                                     L.refine_capacity, L.d_refine_count);
+    e = cudaMemsetAsync(L.d_refine_segs, 0, sizeof(unsigned long long) * (size_t)L.nseg, st);
+    if (e != cudaSuccess)
+        return e;
+    const long long selectBlocks = std::min<long long>((L.npts + 255) / 256, 148LL * 16);
+    refineCountKernel<W><<<(unsigned)selectBlocks, 256, 0, st>>>(L.d_out, L.d_contrib, L.npts, L.nseg,
+                                                                 L.refine_fraction, L.d_refine_segs);
+    refineScanKernel<<<1, 1024, 0, st>>>(L.d_refine_segs, L.nseg, L.work_capacity, L.d_work_count,
+                                         L.d_refined_total);
+    refineSelectKernel<W><<<(unsigned)selectBlocks, 256, 0, st>>>(L.d_out, L.d_contrib, L.npts, L.nseg,
+                                                                  L.refine_fraction, L.d_refine_segs, work,
+                                                                  L.work_capacity);
+    refinePairsKernel64<FIELD><<<148 * CCOIL_FP64_MIN_BLOCKS, 128, 0, st>>>(L.d_blob, L.d_segs, L.d_points, L.d_out,
+                                                                           work, L.work_capacity, L.d_work_count);
     return cudaGetLastError();
 }
 } // namespace
@@ -286,8 +305,6 @@ int launchFields(const FieldLaunch &L, void *stream)
         if (!L.d_work || !L.d_work_count)
             return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "FP32_COMPENSATED needs a near-field work list");
         e = cudaMemsetAsync(L.d_work_count, 0, sizeof(unsigned long long), st);
-        if (e == cudaSuccess && L.d_refine_count)
-            e = cudaMemsetAsync(L.d_refine_count, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess)
             return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(e));
     }

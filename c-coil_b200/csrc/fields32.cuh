@@ -7,15 +7,19 @@
 // list and a second kernel evaluates it with the FP64 integrands, so warps
 // never diverge between the two paths.  If the list is full the pair is
 // integrated in FP64 in place.
+//
+// FP32_REFINED.  The FP32 kernel also stores every (point, segment)
+// contribution; once the point's total is known, a selection kernel removes
+// each contribution whose norm exceeds a set fraction of the total's norm
+// (the contributions that dominate a point where the coils' fields cancel,
+// whose FP32 errors the cancellation magnifies) and lists the pair, and the
+// near-field kernel adds those pairs back evaluated with the FP64 integrands.
 
 #include "integrands32.cuh"
 
-// Integrates one segment for one lane and returns the norm of the lane's
-// contribution (Frobenius norm for the gradient), taken from the cylindrical
-// partial sums before the rotation, which keeps it: the refinement test adds
-// these norms up per point.
+// Integrates one segment for one lane and adds the lane's contribution to acc.
 template <int FIELD, int LANES>
-__device__ __forceinline__ double integrateSegment32(const unsigned char *seg, const Frame &f, int lane, double *acc)
+__device__ __forceinline__ void integrateSegment32(const unsigned char *seg, const Frame &f, int lane, double *acc)
 {
     const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
     const double2 *tt = reinterpret_cast<const double2 *>(seg) + h.off_t;
@@ -26,20 +30,17 @@ __device__ __forceinline__ double integrateSegment32(const unsigned char *seg, c
         double H, Z;
         segmentB32<LANES>(h, tt, lt, pn, f, lane, H, Z);
         addRotated(h, H * f.cphi, H * f.sphi, Z, acc);
-        return sqrt(H * H + Z * Z);
     }
     else if (FIELD == CCOIL_FIELD_G)
     {
         double g[4];
         segmentG32<LANES>(h, tt, lt, pn, f, lane, g);
         addGradient(h, f, g, acc);
-        return sqrt(g[0] * g[0] + g[1] * g[1] + 2.0 * g[2] * g[2] + g[3] * g[3]);
     }
     else
     {
         double a = segmentA32<LANES>(h, tt, lt, pn, f, lane) * h.field_factor;
         addRotated(h, -a * f.sphi, a * f.cphi, 0.0, acc);
-        return fabs(a);
     }
 }
 
@@ -86,14 +87,17 @@ constexpr int fp32MinBlocks(int field)
 #define CCOIL_FP32_STAGE 0
 #endif
 
-template <int FIELD, int LANES>
+// REFINE (FP32_REFINED): every (point, segment) contribution is also written
+// to contrib, segment-major ([segment][point][W], so a warp's stores for one
+// segment are contiguous), near-field pairs as zeros (they are FP64 already)
+template <int FIELD, int LANES, bool REFINE>
 __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(const unsigned char *__restrict__ blob,
                                                       const SegmentDesc *__restrict__ segs, int nseg,
                                                       const double *__restrict__ points, long long npts,
                                                       double *__restrict__ out, NearPair *__restrict__ work,
                                                       unsigned long long workCapacity,
                                                       unsigned long long *__restrict__ workCount,
-                                                      double *__restrict__ cabs)
+                                                      double *__restrict__ contrib)
 {
     constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -128,7 +132,10 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
 #pragma unroll
     for (int i = 0; i < W; ++i)
         acc[i] = 0.0;
-    double cn = 0.0;  // sum of the segments' contribution norms (refinement test)
+    // the lanes of one point
+    auto groupMask = [] {
+        return LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
+    };
 
     for (int s = 0; s < nseg; ++s)
     {
@@ -147,10 +154,44 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
         {
             const SegmentHeader &h = *reinterpret_cast<const SegmentHeader *>(seg);
             const Frame f = toCoilFrame(h, px, py, pz);
-            if (!nearWinding(h, f))
-                cn += integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
+            const bool nearPair = nearWinding(h, f);
+            if (!nearPair && !REFINE)
+                integrateSegment32<FIELD, LANES>(seg, f, lane, acc);
+            else if (!nearPair)
+            {
+                // the segment's contribution on its own: combined over the point's
+                // lanes (all of them take this branch), added to the total by lane 0
+                // and stored for the selection
+                double c[W];
+#pragma unroll
+                for (int i = 0; i < W; ++i)
+                    c[i] = 0.0;
+                integrateSegment32<FIELD, LANES>(seg, f, lane, c);
+#pragma unroll
+                for (int off = LANES / 2; off > 0; off /= 2)
+#pragma unroll
+                    for (int i = 0; i < W; ++i)
+                        c[i] += __shfl_xor_sync(groupMask(), c[i], off);
+                if (lane == 0)
+                {
+                    double *dst = contrib + ((size_t)s * (size_t)npts + (size_t)p) * W;
+#pragma unroll
+                    for (int i = 0; i < W; ++i)
+                    {
+                        acc[i] += c[i];
+                        dst[i] = c[i];
+                    }
+                }
+            }
             else
             {
+                if (REFINE && lane == 0)
+                {
+                    double *dst = contrib + ((size_t)s * (size_t)npts + (size_t)p) * W;
+#pragma unroll
+                    for (int i = 0; i < W; ++i)
+                        dst[i] = 0.0;
+                }
                 bool queued = false;
                 if (lane == 0)
                 {
@@ -163,9 +204,7 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
                     }
                 }
                 // all lanes of the point learn whether the pair was queued
-                const unsigned groupMask = LANES == 32 ? 0xffffffffu
-                                                       : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
-                queued = __shfl_sync(groupMask, queued, (threadIdx.x % 32) / LANES * LANES);
+                queued = __shfl_sync(groupMask(), queued, (threadIdx.x % 32) / LANES * LANES);
                 if (!queued)
                     integrateSegment64Fallback<FIELD, LANES>(seg, px, py, pz, lane, acc);
             }
@@ -196,19 +235,14 @@ __global__ void __launch_bounds__(128, fp32MinBlocks(FIELD)) fieldsKernel32(cons
 
 #pragma unroll
     for (int off = LANES / 2; off > 0; off /= 2)
-    {
 #pragma unroll
         for (int i = 0; i < W; ++i)
             acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
-        cn += __shfl_xor_sync(0xffffffffu, cn, off);
-    }
     if (active && lane == 0)
     {
 #pragma unroll
         for (int i = 0; i < W; ++i)
             out[W * p + i] = acc[i];
-        if (cabs)
-            cabs[p] = cn;
     }
 }
 
@@ -252,73 +286,179 @@ __global__ void __launch_bounds__(256) nearFieldKernel(const unsigned char *__re
     }
 }
 
-// Refinement test: a point whose FP32-evaluated contributions have norms that
-// add up to more than `ratio` times the norm of its total (the coils' fields
-// cancel there, and the total's relative error grows by that ratio; the
-// near-field pairs, evaluated in FP64, do not count) is listed for
-// re-evaluation in FP64.
-template <int W>
-__global__ void __launch_bounds__(256) refineTestKernel(const double *__restrict__ out,
-                                                        const double *__restrict__ cabs, long long npts, double ratio,
-                                                        int *__restrict__ list, unsigned long long capacity,
-                                                        unsigned long long *__restrict__ count)
-{
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npts;
-         p += (long long)gridDim.x * blockDim.x)
-    {
-        double n2 = 0.0;
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-            n2 += out[W * p + k] * out[W * p + k];
-        // !(a <= b) also lists points whose values are not finite
-        if (!(cabs[p] <= ratio * sqrt(n2)))
-        {
-            const unsigned long long slot = atomicAdd(count, 1ull);
-            if (slot < capacity)
-                list[slot] = (int)p;
-        }
-    }
-}
-
-// FP64 re-evaluation of the listed points: all segments with the FP64
-// integrands, LANES threads per point splitting the angular nodes, the result
-// overwriting the point's output.  Grid-stride over the device-side count (no
-// host synchronisation between the passes); a list that overflowed leaves the
-// remaining points at their FP32 values, which the caller learns from the count.
-template <int FIELD, int LANES>
-__global__ void __launch_bounds__(128) refineKernel64(const unsigned char *__restrict__ blob,
-                                                      const SegmentDesc *__restrict__ segs, int nseg,
-                                                      const double *__restrict__ points, double *__restrict__ out,
-                                                      const int *__restrict__ list, unsigned long long capacity,
-                                                      const unsigned long long *__restrict__ count)
+// FP32_REFINED's FP64 pass: one thread per listed (point, segment) pair, the
+// whole segment with the FP64 integrands (so each thickness node's set-up
+// serves all its angular nodes, as in the FP64 field kernel; one warp per pair
+// measured twice the time per pair), the result added to the point's output
+// (FP64 atomics).  Consecutive list entries mostly share their segment (the
+// selection lists a warp's picks of one segment together), so the lanes of a
+// warp run loops of the same length.  Grid-stride over the device-side count.
+template <int FIELD>
+__global__ void __launch_bounds__(128, CCOIL_FP64_MIN_BLOCKS) refinePairsKernel64(
+    const unsigned char *__restrict__ blob, const SegmentDesc *__restrict__ segs, const double *__restrict__ points,
+    double *__restrict__ out, const NearPair *__restrict__ work, unsigned long long workCapacity,
+    const unsigned long long *__restrict__ workCount)
 {
     constexpr int W = FIELD == CCOIL_FIELD_G ? 9 : 3;
-    const unsigned long long n = min(*count, capacity);
-    const int lane = threadIdx.x % LANES;
-    const unsigned long long groups = (unsigned long long)gridDim.x * (blockDim.x / LANES);
-    for (unsigned long long i = (unsigned long long)blockIdx.x * (blockDim.x / LANES) + threadIdx.x / LANES;
-         i < n; i += groups)
+    const unsigned long long n = min(*workCount, workCapacity);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     {
-        const long long p = list[i];
+        const NearPair e = work[i];
+        const long long p = e.point;
         double acc[W];
 #pragma unroll
         for (int k = 0; k < W; ++k)
             acc[k] = 0.0;
-        const double px = points[3 * p], py = points[3 * p + 1], pz = points[3 * p + 2];
+        integrateSegment64<FIELD, 1>(blob + segs[e.segment].offset, points[3 * p], points[3 * p + 1],
+                                     points[3 * p + 2], 0, acc);
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            atomicAdd(&out[W * p + k], acc[k]);
+    }
+}
+
+// FP32_REFINED selection.  A pair is picked when its stored contribution's
+// norm exceeds `fraction` times the norm of the point's total (near-field FP64
+// pairs included); a non-finite total picks nothing.  Both passes below make
+// the same decision from the same data.
+template <int W>
+__device__ __forceinline__ bool refinePick(const double *total, const double *c, double fraction)
+{
+    double n2 = 0.0, c2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < W; ++i)
+    {
+        n2 += total[i] * total[i];
+        c2 += c[i] * c[i];
+    }
+    return c2 > fraction * fraction * n2;
+}
+
+// Pass 1, one thread per point: picks per segment (segCount, zeroed before).
+// Whole warps iterate (base is the warp's first point), so each warp adds once
+// per segment.
+template <int W>
+__global__ void __launch_bounds__(256) refineCountKernel(const double *__restrict__ out,
+                                                         const double *__restrict__ contrib, long long npts, int nseg,
+                                                         double fraction, unsigned long long *__restrict__ segCount)
+{
+    const int lane = threadIdx.x % 32;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < npts; base += stride)
+    {
+        const long long p = base + lane;
+        const bool active = p < npts;
+        double total[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            total[i] = active ? out[W * p + i] : 0.0;
         for (int s = 0; s < nseg; ++s)
-            integrateSegment64<FIELD, LANES>(blob + segs[s].offset, px, py, pz, lane, acc);
-        const unsigned groupMask = LANES == 32 ? 0xffffffffu
-                                               : (((1u << LANES) - 1u) << ((threadIdx.x % 32) / LANES * LANES));
+        {
+            double c[W];
 #pragma unroll
-        for (int off = LANES / 2; off > 0; off /= 2)
+            for (int i = 0; i < W; ++i)
+                c[i] = active ? contrib[((size_t)s * (size_t)npts + (size_t)p) * W + i] : 0.0;
+            const unsigned mask = __ballot_sync(0xffffffffu, active && refinePick<W>(total, c, fraction));
+            if (mask != 0u && lane == 0)
+                atomicAdd(&segCount[s], (unsigned long long)__popc(mask));
+        }
+    }
+}
+
+// Pass 2, one block: segCount becomes each segment's first list slot (exclusive
+// prefix sum in segment order), *count the number of picks (the list length,
+// read by the FP64 pass), *refined grows by the picks that fit the list.
+__global__ void __launch_bounds__(1024) refineScanKernel(unsigned long long *__restrict__ segCount, int nseg,
+                                                         unsigned long long capacity,
+                                                         unsigned long long *__restrict__ count,
+                                                         unsigned long long *__restrict__ refined)
+{
+    __shared__ unsigned long long part[1024];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nseg; base += 1024)
+    {
+        const int s = base + threadIdx.x;
+        const unsigned long long v = s < nseg ? segCount[s] : 0ull;
+        part[threadIdx.x] = v;
+        __syncthreads();
+        // Hillis-Steele inclusive scan of the block's slice
+        for (int off = 1; off < 1024; off *= 2)
+        {
+            const unsigned long long add = threadIdx.x >= off ? part[threadIdx.x - off] : 0ull;
+            __syncthreads();
+            part[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (s < nseg)
+            segCount[s] = carry + part[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            carry += part[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        *count = carry;
+        *refined += carry < capacity ? carry : capacity;
+    }
+}
+
+// Pass 3, one thread per point: every picked pair takes the next slot of its
+// segment's range (one atomic per warp and segment), is listed if the slot
+// fits the list, and then leaves the point's total; the list comes out
+// segment-major, so the FP64 pass's warps read one segment's tables.
+template <int W>
+__global__ void __launch_bounds__(256) refineSelectKernel(double *__restrict__ out,
+                                                          const double *__restrict__ contrib, long long npts, int nseg,
+                                                          double fraction, unsigned long long *__restrict__ segNext,
+                                                          NearPair *__restrict__ work, unsigned long long capacity)
+{
+    const int lane = threadIdx.x % 32;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < npts; base += stride)
+    {
+        const long long p = base + lane;
+        const bool active = p < npts;
+        double total[W], picked[W];
 #pragma unroll
-            for (int k = 0; k < W; ++k)
-                acc[k] += __shfl_xor_sync(groupMask, acc[k], off);
-        if (lane == 0)
+        for (int i = 0; i < W; ++i)
+        {
+            total[i] = active ? out[W * p + i] : 0.0;
+            picked[i] = 0.0;
+        }
+        for (int s = 0; s < nseg; ++s)
+        {
+            double c[W];
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                c[i] = active ? contrib[((size_t)s * (size_t)npts + (size_t)p) * W + i] : 0.0;
+            const bool pick = active && refinePick<W>(total, c, fraction);
+            const unsigned mask = __ballot_sync(0xffffffffu, pick);
+            if (mask == 0u)
+                continue;
+            unsigned long long first = 0;
+            if (lane == 0)
+                first = atomicAdd(&segNext[s], (unsigned long long)__popc(mask));
+            first = __shfl_sync(0xffffffffu, first, 0);
+            const unsigned long long slot = first + (unsigned long long)__popc(mask & ((1u << lane) - 1u));
+            if (pick && slot < capacity)
+            {
+                work[slot].point = (int)p;
+                work[slot].segment = s;
+#pragma unroll
+                for (int i = 0; i < W; ++i)
+                    picked[i] += c[i];
+            }
+        }
+        if (active)
         {
 #pragma unroll
-            for (int k = 0; k < W; ++k)
-                out[W * p + k] = acc[k];
+            for (int i = 0; i < W; ++i)
+                out[W * p + i] = total[i] - picked[i];
         }
     }
 }

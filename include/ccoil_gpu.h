@@ -49,11 +49,11 @@ typedef enum ccoil_status
 /* Arithmetic of the quadrature.  FP64 reproduces the reference's double CPU
  * path; FP32_COMPENSATED runs the bulk of the nodes in FP32 with compensated
  * accumulation and keeps FP64 for near-field points and the final sums;
- * FP32_REFINED (fields) is FP32_COMPENSATED followed by an FP64 re-evaluation
- * of every point where the coils' fields cancel, i.e. where the norms of the
- * FP32-evaluated contributions add up to more than a set ratio times the norm
- * of the total (ccoil_set_refine_ratio; the total's relative error grows by
- * that ratio). */
+ * FP32_REFINED (field plans) is FP32_COMPENSATED in which every (point, coil)
+ * contribution whose norm exceeds a set fraction of the norm of the point's
+ * total is replaced by its FP64 value (ccoil_set_refine_fraction): where the
+ * coils' fields cancel, the contributions that dominate carry errors that the
+ * cancellation magnifies, and those are re-evaluated. */
 typedef enum ccoil_precision
 {
     CCOIL_PRECISION_FP64 = 0,
@@ -181,14 +181,17 @@ int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
 int ccoil_set_point_ordering(int enabled);
 int ccoil_point_ordering(void);
 
-/* FP32_REFINED's test ratio (process-wide, read when a plan executes; >= 1):
- * a point is re-evaluated in FP64 when the norms of its FP32-evaluated
- * contributions add up to more than `ratio` times the norm of its total.
- * Smaller ratios refine more points; the default is 10.  ccoil_field_plan_refined_points reports
- * how many points the plan's last execution re-evaluated (synchronous). */
-int ccoil_set_refine_ratio(double ratio);
-double ccoil_refine_ratio(void);
-int ccoil_field_plan_refined_points(ccoil_field_plan_t *plan, long long *count);
+/* FP32_REFINED's fraction (process-wide, read when a plan executes; finite,
+ * >= 0; default 0.1): a (point, coil segment) pair is re-evaluated in FP64 when
+ * the norm of its FP32 contribution exceeds `fraction` times the norm of the
+ * point's total.  Smaller fractions refine more pairs; 0 refines every pair
+ * with a non-zero contribution.  The plan stores every contribution of a chunk
+ * of points (at most 2 GiB; larger calls run in several chunks).  Points with
+ * a non-finite total are not refined.  ccoil_field_plan_refined_pairs reports
+ * how many pairs the plan's last execution re-evaluated (synchronous). */
+int ccoil_set_refine_fraction(double fraction);
+double ccoil_refine_fraction(void);
+int ccoil_field_plan_refined_pairs(ccoil_field_plan_t *plan, long long *count);
 
 /* ------------------------------------------------------------------------ *
  * Coil pairs over many arrangements                                         *

@@ -187,44 +187,72 @@ def test_mirror_pair_tables(ccoil, angular):
 
 
 def test_refined_mode(ccoil):
-    """FP32_REFINED re-evaluates in FP64 every point whose FP32 contributions' norms add
-    up to more than the set ratio times its total's norm: with a ratio of 1 (every
-    point qualifies, the sum of norms is never below the norm of the sum) the result
-    is, at nearly every point, the FP64 result up to summation order (a point whose
-    contributions are all near-field pairs, already FP64, or exactly parallel need
-    not qualify); with a larger ratio only the
-    cancelling points are re-evaluated and the error is never above FP32_COMPENSATED's
-    at any point that was re-evaluated."""
+    """FP32_REFINED replaces by its FP64 value every (point, coil) contribution whose
+    norm exceeds the set fraction of the point's total.  With fraction 0 every pair
+    is FP64 and the result is the FP64 path's up to summation order; at the default
+    0.1 the maximum error of A, B and E falls below 1e-7 on the 16-coil group
+    (from the FP32 path's 4-6e-7), with part of the pairs refined; the gradient
+    stays within its FP32 bars.  Fractions must be finite and
+    >= 0."""
     import ctypes
     from ccoil_b200 import workloads
     L = ccoil.lib()
-    default = L.ccoil_refine_ratio()
+    default = L.ccoil_refine_fraction()
+    assert default == 0.1
     rows = workloads.coil_rows_mixed(16, seed=77)
     pts = workloads.points_cube(8192, seed=78)
     coils = workloads.coils_from_rows(rows, 5.0)
+    near = np.zeros(len(pts), dtype=bool)
     try:
-        for field in (0, 1, 3):
+        for field in (0, 1, 2, 3):
             f64 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP64)
             f32 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
-            L.ccoil_set_refine_ratio(ctypes.c_double(1.0))
+            L.ccoil_set_refine_fraction(ctypes.c_double(0.0))
             plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_REFINED)
             got = plan(pts)
-            n_all = plan.refined_points()
+            n_all = plan.refined_pairs()
             plan.close()
-            e = rel_err(got, f64)
-            assert n_all >= 0.9 * len(pts) and np.sum(e < 1e-13) >= n_all, (field, n_all, np.sum(e < 1e-13))
-            L.ccoil_set_refine_ratio(ctypes.c_double(3.0))
+            assert 0.9 * len(pts) * len(coils) <= n_all <= len(pts) * len(coils), (field, n_all)
+            assert rel_err(got, f64).max() < 1e-13, (field, rel_err(got, f64).max())
+            L.ccoil_set_refine_fraction(ctypes.c_double(default))
             plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_REFINED)
             got = plan(pts)
-            n = plan.refined_points()
+            n = plan.refined_pairs()
             plan.close()
-            assert 0 < n < len(pts)
-            e, e32 = rel_err(got, f64), rel_err(f32, f64)
-            redone = e < 1e-13
-            assert redone.sum() >= n and e.max() <= e32.max(), (field, n, e.max(), e32.max())
+            # with 16 coils each coil's share of a point's field is large: about
+            # half of the pairs exceed 0.1 of the total (12 % on the 128-coil group)
+            assert 0 < n < 0.7 * len(pts) * len(coils), (field, n)
+            keep = ~gradient_band(rows, pts) if field == 3 else ~near
+            e, e32 = rel_err(got, f64)[keep], rel_err(f32, f64)[keep]
+            print(field, "refined pairs %.3f, max %.1e (FP32c %.1e), p99 %.1e" %
+                  (n / (len(pts) * len(coils)), e.max(), e32.max(), np.quantile(e, 0.99)))
+            if field == 3:
+                assert np.median(e) < 1e-7 and e.max() < 1e-6, (field, e.max())
+            else:
+                assert e.max() < 1e-7 and e.max() < e32.max() / 3, (field, e.max(), e32.max())
     finally:
-        L.ccoil_set_refine_ratio(ctypes.c_double(default))
-    assert L.ccoil_set_refine_ratio(ctypes.c_double(0.5)) == 1
+        L.ccoil_set_refine_fraction(ctypes.c_double(default))
+    assert L.ccoil_set_refine_fraction(ctypes.c_double(-0.5)) == 1
+    assert L.ccoil_set_refine_fraction(ctypes.c_double(float("nan"))) == 1
+    assert L.ccoil_refine_fraction() == default
+
+
+def test_refined_mode_in_chunks(ccoil):
+    """FP32_REFINED stores every contribution of the points it evaluates at once: a
+    gradient call whose contributions exceed 2 GiB (80 coils x 420,000 points x 9
+    doubles) runs in several chunks and matches FP64 like a single chunk does."""
+    from ccoil_b200 import workloads
+    rows = workloads.coil_rows_mixed(80, seed=91)
+    pts = workloads.points_cube(420000, seed=92)
+    coils = workloads.coils_from_rows(rows, 3.0)
+    f64 = evaluate(ccoil, coils, pts, 3, ccoil.PrecisionMode.FP64)
+    plan = ccoil.FieldPlan([c.struct() for c in coils], 3, ccoil.PrecisionMode.FP32_REFINED)
+    got = plan(pts)
+    n = plan.refined_pairs()
+    plan.close()
+    e = rel_err(got, f64)[~gradient_band(rows, pts)]
+    assert 0 < n < 0.5 * len(pts) * len(coils), n
+    assert np.median(e) < 1e-9 and e.max() < 1e-6, (np.median(e), e.max())
 
 
 def test_point_ordering(ccoil):
