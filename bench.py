@@ -6,8 +6,13 @@ I ~ U[-5, 5] A, centres in a 1 m cube, random axes) at 2^20 points per GPU
 (uniform in a 2 m cube), PrecisionFactor 5, every coil at its CPU
 PrecisionArguments.  Seeded synthetic data; no dataset is involved.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32c|both]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32c|fp32r|both|all]
     python bench.py --impl reference        # the reference's own CPU_MT code on this host
+    python bench.py --workload refine-sweep # FP32_REFINED's cost and error over its fraction
+
+The headline configuration (fp32r) is the FP32 one whose maximum error away
+from windings stays below 1e-7: FP32_REFINED for A and B, FP32_COMPENSATED
+for G; fp64 and fp32c (FP32_COMPENSATED for every field) are timed beside it.
     python bench.py --workload batched      # 2,048 independent systems, one persistent launch per step
     python bench.py --workload adjoint      # forward + backward of a B-field loss (64 coils)
     python bench.py --workload pf-sweep     # the group at PrecisionFactor 1, 3, 5, 7, 9
@@ -40,7 +45,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="both", choices=["fp64", "fp32c", "both"])
+    ap.add_argument("--precision", default="all", choices=["fp64", "fp32c", "fp32r", "both", "all"],
+                    help="fp32r: FP32_REFINED for A and B, FP32_COMPENSATED for G (the configuration at "
+                         "<= 1e-7); both: fp64 + fp32c; all: fp64 + fp32c + fp32r (headline fp32r)")
     ap.add_argument("--points", type=int, default=1 << 20)
     ap.add_argument("--coils", type=int, default=128)
     ap.add_argument("--pf", type=float, default=5.0)
@@ -435,7 +442,7 @@ def bench_pf_sweep(a):
             "config": {"workload": "coil group: 128 mixed coils, 262144 points in a 2 m cube, A+B+G, "
                                    "PrecisionFactor 1, 3, 5, 7, 9 (value: PF 5)", "coils": a.coils,
                        "points": npts, "l2": "flushed between timed launches (256 MiB write)"},
-            "sweep": sweep, "gpu_launches": (field_launches(0, npts) + field_launches(1, npts)) * len(FIELDS) * a.steps * 5}
+            "sweep": sweep, "gpu_launches": (field_launches(0, npts, 1, 0) + field_launches(1, npts, 1, 0)) * len(FIELDS) * a.steps * 5}
     print(json.dumps(line))
 
 
@@ -547,13 +554,28 @@ def main():
     group = cc.CoilGroup(coils, cc.PrecisionFactor(a.pf))
     pts_host = workloads.points_cube(a.points, seed=1000 + 2 + 7919 * rank)
     pts = torch.from_numpy(pts_host).to(dev)
-    modes = {"fp64": [cc.PrecisionMode.FP64], "fp32c": [cc.PrecisionMode.FP32_COMPENSATED],
-             "both": [cc.PrecisionMode.FP64, cc.PrecisionMode.FP32_COMPENSATED]}[a.precision]
+    PM = cc.PrecisionMode
+    # precision configurations: one mode per field.  fp32r is the one whose maximum
+    # error away from windings stays below 1e-7: FP32_REFINED for A and B, whose FP32
+    # errors the coils' cancellation magnifies past it, FP32_COMPENSATED for G, whose
+    # FP32 error is two orders lower
+    configs = {"fp64": {"A": PM.FP64, "B": PM.FP64, "G": PM.FP64},
+               "fp32c": {"A": PM.FP32_COMPENSATED, "B": PM.FP32_COMPENSATED, "G": PM.FP32_COMPENSATED},
+               "fp32r": {"A": PM.FP32_REFINED, "B": PM.FP32_REFINED, "G": PM.FP32_COMPENSATED}}
+    selected = {"fp64": ["fp64"], "fp32c": ["fp32c"], "fp32r": ["fp32r"], "both": ["fp64", "fp32c"],
+                "all": ["fp64", "fp32c", "fp32r"]}[a.precision]
+    headline = "fp32r" if "fp32r" in selected else ("fp32c" if "fp32c" in selected else "fp64")
+    modes = [m for m in (PM.FP64, PM.FP32_COMPENSATED)
+             if ("fp64" in selected if m == PM.FP64 else ("fp32c" in selected or "fp32r" in selected))]
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     results = {}
-    for mode in modes:
-        plans = {name: group.plan(f, mode) for name, f in FIELDS}
+    launches = {}
+    for key in selected:
+        cfg = configs[key]
+        plans = {name: group.plan(f, cfg[name]) for name, f in FIELDS}
+        launches[key] = sum(field_launches(cfg[name], a.points, plans[name].segment_count(), f)
+                            for name, f in FIELDS)
         outs = {name: torch.empty((a.points, 9 if f == 3 else 3), dtype=torch.float64, device=dev)
                 for name, f in FIELDS}
         for _ in range(max(a.warmup, 3)):
@@ -580,8 +602,8 @@ def main():
         barrier()
         step_ms = max_over_ranks(step_ms / a.steps)
         field_ms = {k: max_over_ranks(v / a.steps) for k, v in field_ms.items()}
-        results[int(mode)] = {"step_ms": step_ms, "field_ms": field_ms, "clocks": clk.summary(),
-                              "outs": {k: v.clone() for k, v in outs.items()}}
+        results[key] = {"step_ms": step_ms, "field_ms": field_ms, "clocks": clk.summary(),
+                        "outs": {k: v.clone() for k, v in outs.items()}}
 
         # end to end through the public API: pinned host points in, pinned host results out
         pin_pts = torch.from_numpy(pts_host).pin_memory()
@@ -595,36 +617,40 @@ def main():
             for name, _f in FIELDS:
                 plans[name](pin_pts.numpy(), out=pin_out[name].numpy())
         e2e_s = max_over_ranks((time.perf_counter() - t0) / a.steps)
-        results[int(mode)]["e2e_s"] = e2e_s
+        results[key]["e2e_s"] = e2e_s
         for p in plans.values():
             p.close()
         # one-shot calls, the reference glue's pattern (ccoil_compute_fields): every call
         # builds and uploads the node tables, copies the points in and the results out
         api = {"A": group.compute_all_A_potential_vectors, "B": group.compute_all_B_field_vectors,
                "G": group.compute_all_B_gradient_matrices}
-        api["A"](pin_pts.numpy(), precision_mode=mode)
+        api["A"](pin_pts.numpy(), precision_mode=cfg["A"])
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         for _ in range(a.steps):
             for name, _f in FIELDS:
-                api[name](pin_pts.numpy(), precision_mode=mode)
-        results[int(mode)]["e2e_oneshot_s"] = max_over_ranks((time.perf_counter() - t0) / a.steps)
+                api[name](pin_pts.numpy(), precision_mode=cfg[name])
+        results[key]["e2e_oneshot_s"] = max_over_ranks((time.perf_counter() - t0) / a.steps)
 
     units_per_step = len(FIELDS) * a.coils * a.points * world
-    headline_mode = int(modes[-1])
-    r = results[headline_mode]
+    r = results[headline]
     value = units_per_step / (r["step_ms"] * 1e-3)
     e2e_value = units_per_step / r["e2e_s"]
+    # the roofline's kernel: the longest single launch, the FP32-compensated field
+    # kernel of the slowest field (FP32_REFINED splits its work over chunks and passes)
+    roof_key = "fp32c" if "fp32c" in results else headline
+    headline_mode = 0 if roof_key == "fp64" else 1
+    rr = results[roof_key]
 
     # roofline of the dominant kernel: its algorithmic work (the reference's operations
     # per node, each add, multiply, divide, square root or logarithm one flop) over its
     # CUDA-event time, against the measured FMA peak (2 flops per FMA) of the pipe it
     # runs on; the instruction-issue and MUFU models are reported beside it
     rates = ctypes_rates(cc)
-    dom = max(r["field_ms"], key=r["field_ms"].get)
+    dom = max(rr["field_ms"], key=rr["field_ms"].get)
     fidx = dict(FIELDS)[dom]
-    t_dom = r["field_ms"][dom] * 1e-3
+    t_dom = rr["field_ms"][dom] * 1e-3
     flops_launch = opcount.group_flops_per_point(fidx, coils) * a.points
     model = {"algorithmic_flops_per_launch": flops_launch}
     if rates is None:
@@ -654,11 +680,13 @@ def main():
             "warmup": a.warmup, "ms_per_step": r["step_ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if headline_mode == 0 else "f32 (compensated) + f64",
             "data": "synthetic (seeded)", "config": workload_config(a, world),
-            "precision_mode": "fp64" if headline_mode == 0 else "fp32c",
+            "precision_mode": {"fp64": "fp64", "fp32c": "fp32c (FP32_COMPENSATED, every field)",
+                               "fp32r": "fp32r: FP32_REFINED for A and B (fraction %g), FP32_COMPENSATED for G"
+                                        % cc.lib().ccoil_refine_fraction()}[headline],
             "per_field_ms": r["field_ms"],
             "node_evals_per_s": opcount.group_nodes_per_point(coils) * a.points * world * len(FIELDS) /
             (r["step_ms"] * 1e-3),
-            "gpu_launches": a.steps * len(FIELDS) * field_launches(headline_mode, a.points),
+            "gpu_launches": a.steps * launches[headline],
             "clocks": r["clocks"],
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": len(FIELDS) * a.points * 24,
@@ -667,7 +695,8 @@ def main():
             "e2e_one_shot": {"value": units_per_step / r["e2e_oneshot_s"], "unit": UNIT,
                              "path": "CoilGroup.compute_all_* (ccoil_compute_fields): node tables built and "
                                      "uploaded, points copied in and results out on every call"},
-            "roofline": {"bound": bound, "kernel": "field %s" % dom, "achieved": achieved, "peak": peak,
+            "roofline": {"bound": bound, "kernel": "field %s, %s" % (dom, configs[roof_key][dom].name),
+                         "achieved": achieved, "peak": peak,
                          "unit": unit, "frac": (achieved / peak) if peak else None, "traffic": traffic,
                          "peak_source": "measured on this GPU by ccoil_measure_op_rates (FMA = 2 flops); "
                                         "achieved counts the reference's operations, one flop each",
@@ -677,22 +706,29 @@ def main():
                              "fp64_fma_tflops": 2 * rates[0] / 1e12, "fp32_fma_tflops": 2 * rates[4] / 1e12,
                              "mufu_tops": rates[5] / 1e12, "ddiv_gops": rates[1] / 1e9,
                              "dsqrt_gops": rates[2] / 1e9, "dlog_gops": rates[3] / 1e9}}}
-    if len(modes) == 2:
-        r64 = results[0]
-        line["fp64"] = {"value": units_per_step / (r64["step_ms"] * 1e-3), "ms_per_step": r64["step_ms"],
-                        "per_field_ms": r64["field_ms"]}
-        line["fp32c_speedup_vs_fp64"] = r64["step_ms"] / r["step_ms"]
+    for key in selected:
+        rk = results[key]
+        line[key] = {"value": units_per_step / (rk["step_ms"] * 1e-3), "ms_per_step": rk["step_ms"],
+                     "per_field_ms": rk["field_ms"], "e2e": units_per_step / rk["e2e_s"],
+                     "e2e_one_shot": units_per_step / rk["e2e_oneshot_s"],
+                     "modes": {name: configs[key][name].name for name, _f in FIELDS}}
+    if "fp64" in results:
+        r64 = results["fp64"]
         near, band = (torch.from_numpy(m).to(dev) for m in winding_masks(rows, pts_host))
-        errs = {"definition": "norm-wise relative error per point, denominator floored at 1e-3 x the batch's "
-                              "largest FP64 norm; 'away' = outside every coil's winding box inflated by 0.1 R "
-                              "(for G also outside every coil's radial band [0.9 R, R + a + 0.1 R], where the "
-                              "reference's FP64 gradient is itself ill-conditioned)",
-                "away_fraction": {"A_B": float((~near).float().mean()), "G": float((~band).float().mean())}}
-        for name, f in FIELDS:
-            away = ~band if f == 3 else ~near
-            errs[name] = {"all": rel_err_stats(results[1]["outs"][name], r64["outs"][name]),
-                          "away": rel_err_stats(results[1]["outs"][name], r64["outs"][name], away)}
-        line["fp32c_rel_err_vs_fp64"] = errs
+        for key in ("fp32c", "fp32r"):
+            if key not in results:
+                continue
+            line[key + "_speedup_vs_fp64"] = r64["step_ms"] / results[key]["step_ms"]
+            errs = {"definition": "norm-wise relative error per point, denominator floored at 1e-3 x the batch's "
+                                  "largest FP64 norm; 'away' = outside every coil's winding box inflated by 0.1 R "
+                                  "(for G also outside every coil's radial band [0.9 R, R + a + 0.1 R], where the "
+                                  "reference's FP64 gradient is itself ill-conditioned)",
+                    "away_fraction": {"A_B": float((~near).float().mean()), "G": float((~band).float().mean())}}
+            for name, f in FIELDS:
+                away = ~band if f == 3 else ~near
+                errs[name] = {"all": rel_err_stats(results[key]["outs"][name], r64["outs"][name]),
+                              "away": rel_err_stats(results[key]["outs"][name], r64["outs"][name], away)}
+            line[key + "_rel_err_vs_fp64"] = errs
     if a.arrangements > 0:
         arr = bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, modes)
         head = "fp32c" if "fp32c" in arr else "fp64"
@@ -755,14 +791,23 @@ def ctypes_rates(cc):
     return list(v)
 
 
-def field_launches(mode, points):
+def field_launches(mode, points, segments, field):
     """Kernel launches of one field-plan evaluation: FP64 one field kernel; FP32c the field
     kernel and its near-field FP64 pass, and from 16,384 to 2^30 points also the point
     ordering (bounds, Morton keys, the radix sort's 6 kernels, gather) and the scatter of
-    the results."""
-    if int(mode) == 0:
+    the results; FP32_REFINED per chunk of points (contributions of at most 4 GiB, at most
+    2^28 listed pairs) the field kernel, the near-field pass and the selection (count,
+    scan, select) and FP64 pair passes."""
+    mode = int(mode)
+    if mode == 0:
         return 1
-    return 2 + (10 if (1 << 14) <= points <= (1 << 30) else 0)
+    ordering = 10 if (1 << 14) <= points <= (1 << 30) else 0
+    if mode == 1:
+        return 2 + ordering
+    width = 9 if field == 3 else 3
+    per_chunk = min((1 << 32) // (segments * width * 8), (1 << 28) // segments)
+    chunks = -(-points // max(1, per_chunk))
+    return ordering + 6 * chunks
 
 
 def read_profile(field, mode):

@@ -84,6 +84,7 @@ def lib():
     L.ccoil_field_plan_create.argtypes = [cp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.ccoil_field_plan_execute.argtypes = [vp, vp, ctypes.c_longlong, vp, ctypes.c_int, ctypes.c_int, vp]
     L.ccoil_field_plan_destroy.argtypes = [vp]
+    L.ccoil_field_plan_segment_count.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.ccoil_timeout_count.restype = ctypes.c_longlong
     L.ccoil_check_bounded_wait.argtypes = [ctypes.c_longlong, vp]
     L.ccoil_set_point_ordering.argtypes = [ctypes.c_int]

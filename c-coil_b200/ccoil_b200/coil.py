@@ -178,6 +178,13 @@ class FieldPlan:
                                              ctypes.c_void_p(stream or 0)))
         return res
 
+    def segment_count(self):
+        """Segments the plan evaluates per point (one per coil, more for coils whose
+        node tables exceed one segment)."""
+        n = ctypes.c_int()
+        check(lib().ccoil_field_plan_segment_count(self._h, ctypes.byref(n)))
+        return n.value
+
     def refined_pairs(self):
         """(point, coil segment) pairs the last execution re-evaluated in FP64
         (FP32_REFINED plans)."""

@@ -428,6 +428,14 @@ int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, lon
     return CCOIL_OK;
 }
 
+int ccoil_field_plan_segment_count(const ccoil_field_plan_t *plan, int *count)
+{
+    if (!plan || !count)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "null plan or count");
+    *count = (int)plan->set.segs.size();
+    return CCOIL_OK;
+}
+
 int ccoil_field_plan_destroy(ccoil_field_plan_t *plan)
 {
     if (!plan)

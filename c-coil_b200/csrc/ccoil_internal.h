@@ -192,9 +192,11 @@ constexpr size_t kNearPairBytes = 8;
 // and brings the maximum relative error of A and B below 1e-7
 constexpr double kDefaultRefineFraction = 0.1;
 // FP32_REFINED evaluates the points in chunks whose stored contributions fit
-// this many bytes, and lists at most kRefineListPairs pairs per chunk
-constexpr size_t kRefineContribBytes = size_t(1) << 31;
-constexpr unsigned long long kRefineListPairs = 1ULL << 25;
+// this many bytes (the 128-coil benchmark group's A and B at 2^20 points take
+// 3.8 GB: one chunk), and lists at most kRefineListPairs pairs per chunk (8
+// bytes each; every pair of a chunk of A, B or E fits)
+constexpr size_t kRefineContribBytes = size_t(1) << 32;
+constexpr unsigned long long kRefineListPairs = 1ULL << 28;
 int launchFields(const FieldLaunch &L, void *stream);
 int readTimeouts(long long &count);
 

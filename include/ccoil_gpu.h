@@ -168,6 +168,10 @@ int ccoil_field_plan_create(const ccoil_coil_t *coils, int coil_count, int field
 int ccoil_field_plan_execute(ccoil_field_plan_t *plan, const double *points, long long point_count, double *out,
                              int memory, int lanes_per_point, void *stream);
 int ccoil_field_plan_destroy(ccoil_field_plan_t *plan);
+/* Number of segments (a coil's geometry with a slice of its node tables; a
+ * coil whose tables exceed one staging buffer spans several) the plan
+ * evaluates per point. */
+int ccoil_field_plan_segment_count(const ccoil_field_plan_t *plan, int *count);
 
 /* Point ordering of the FP32 plans (process-wide, read when a plan executes;
  * on by default): an FP32_COMPENSATED or FP32_REFINED plan given at least
@@ -186,7 +190,8 @@ int ccoil_point_ordering(void);
  * the norm of its FP32 contribution exceeds `fraction` times the norm of the
  * point's total.  Smaller fractions refine more pairs; 0 refines every pair
  * with a non-zero contribution.  The plan stores every contribution of a chunk
- * of points (at most 2 GiB; larger calls run in several chunks).  Points with
+ * of points (at most 4 GiB, plus a list of at most 2 GiB; larger calls run in
+ * several chunks).  Points with
  * a non-finite total are not refined.  ccoil_field_plan_refined_pairs reports
  * how many pairs the plan's last execution re-evaluated (synchronous). */
 int ccoil_set_refine_fraction(double fraction);

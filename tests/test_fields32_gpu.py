@@ -239,11 +239,11 @@ def test_refined_mode(ccoil):
 
 def test_refined_mode_in_chunks(ccoil):
     """FP32_REFINED stores every contribution of the points it evaluates at once: a
-    gradient call whose contributions exceed 2 GiB (80 coils x 420,000 points x 9
+    gradient call whose contributions exceed 4 GiB (128 coils x 500,000 points x 9
     doubles) runs in several chunks and matches FP64 like a single chunk does."""
     from ccoil_b200 import workloads
-    rows = workloads.coil_rows_mixed(80, seed=91)
-    pts = workloads.points_cube(420000, seed=92)
+    rows = workloads.coil_rows_mixed(128, seed=91)
+    pts = workloads.points_cube(500000, seed=92)
     coils = workloads.coils_from_rows(rows, 3.0)
     f64 = evaluate(ccoil, coils, pts, 3, ccoil.PrecisionMode.FP64)
     plan = ccoil.FieldPlan([c.struct() for c in coils], 3, ccoil.PrecisionMode.FP32_REFINED)
