@@ -180,7 +180,7 @@ def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, mod
     ds = torch.from_numpy(sposes).to(dev)
     res = {}
     for mode in modes:
-        key = "fp64" if int(mode) == 0 else "fp32c"
+        key = {0: "fp64", 1: "fp32c", 2: "fp32r"}[int(mode)]
         res[key] = {}
         for name, q, w in (("M", 0, 1), ("FT", 1, 6)):
             out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
@@ -198,11 +198,13 @@ def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, mod
             ms = max_over_ranks(ms / a.steps)
             res[key][name] = {"ms": ms, "arrangements_per_s": a.arrangements / (ms * 1e-3), "z_axis_cases": zc,
                               "out": out}
-    if len(res) == 2:
-        m32, m64 = res["fp32c"]["M"]["out"], res["fp64"]["M"]["out"]
-        f32, f64 = res["fp32c"]["FT"]["out"], res["fp64"]["FT"]["out"]
-        res["errors"] = {"M": rel_err_stats(m32, m64), "F": rel_err_stats(f32[:, :3], f64[:, :3]),
-                         "T": rel_err_stats(f32[:, 3:], f64[:, 3:])}
+    if "fp64" in res:
+        m64, f64 = res["fp64"]["M"]["out"], res["fp64"]["FT"]["out"]
+        for key in ("fp32c", "fp32r"):
+            if key in res:
+                m32, f32 = res[key]["M"]["out"], res[key]["FT"]["out"]
+                res[key + "_errors"] = {"M": rel_err_stats(m32, m64), "F": rel_err_stats(f32[:, :3], f64[:, :3]),
+                                        "T": rel_err_stats(f32[:, 3:], f64[:, 3:])}
     aB, tB, lB, aI, tI, lI = sp.as_tuple()
     res["secondary_nodes"] = aB * aI * tB * tI * lB * lI
     res["primary_nodes"] = pp.angular_blocks * pp.angular_increments * pp.thickness_blocks * pp.thickness_increments
@@ -565,8 +567,9 @@ def main():
     selected = {"fp64": ["fp64"], "fp32c": ["fp32c"], "fp32r": ["fp32r"], "both": ["fp64", "fp32c"],
                 "all": ["fp64", "fp32c", "fp32r"]}[a.precision]
     headline = "fp32r" if "fp32r" in selected else ("fp32c" if "fp32c" in selected else "fp64")
-    modes = [m for m in (PM.FP64, PM.FP32_COMPENSATED)
-             if ("fp64" in selected if m == PM.FP64 else ("fp32c" in selected or "fp32r" in selected))]
+    # arrangement precisions: FP64, FP32_COMPENSATED and FP32_REFINED as selected
+    modes = [m for m, key in ((PM.FP64, "fp64"), (PM.FP32_COMPENSATED, "fp32c"), (PM.FP32_REFINED, "fp32r"))
+             if key in selected]
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     results = {}
@@ -731,7 +734,7 @@ def main():
             line[key + "_rel_err_vs_fp64"] = errs
     if a.arrangements > 0:
         arr = bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, modes)
-        head = "fp32c" if "fp32c" in arr else "fp64"
+        head = "fp32c" if "fp32c" in arr else ("fp32r" if "fp32r" in arr else "fp64")
         line["arrangements"] = {"workload": "RECTANGULAR primary (0.1, 0.05, 0.1 m, N=200) x THIN secondary "
                                             "(0.05, 0, 0.2 m, N=100), %d arrangements per GPU, offsets in a "
                                             "0.6 m cube, random orientations, 5%% near-coaxial, PF 5"
@@ -741,16 +744,23 @@ def main():
                                 "FT_arrangements_per_s": arr[head]["FT"]["arrangements_per_s"] * world,
                                 "secondary_nodes": arr["secondary_nodes"], "primary_nodes": arr["primary_nodes"],
                                 "z_axis_cases": arr[head]["M"]["z_axis_cases"]}
-        for key in ("fp64", "fp32c"):
+        for key in ("fp64", "fp32c", "fp32r"):
             if key in arr:
                 line["arrangements"][key] = {
                     "M_arrangements_per_s": arr[key]["M"]["arrangements_per_s"] * world,
                     "FT_arrangements_per_s": arr[key]["FT"]["arrangements_per_s"] * world,
                     "M_ms": arr[key]["M"]["ms"], "FT_ms": arr[key]["FT"]["ms"]}
-        if "errors" in arr:
-            line["arrangements"]["fp32c_speedup_vs_fp64"] = {
-                q: arr["fp64"][q]["ms"] / arr["fp32c"][q]["ms"] for q in ("M", "FT")}
-            line["arrangements"]["fp32c_rel_err_vs_fp64"] = arr["errors"]
+            if key + "_errors" in arr:
+                line["arrangements"][key + "_speedup_vs_fp64"] = {
+                    q: arr["fp64"][q]["ms"] / arr[key][q]["ms"] for q in ("M", "FT")}
+                line["arrangements"][key + "_rel_err_vs_fp64"] = arr[key + "_errors"]
+        if "fp64" in arr:
+            # no FP32 form reaches 1e-7 on every arrangement at less than FP64's cost
+            # (FP32_REFINED needs a fraction near 0.005 for it): the 1e-7 figure is FP64's
+            line["arrangements"]["at_1e-7"] = {
+                "precision_mode": "fp64",
+                "M_arrangements_per_s": arr["fp64"]["M"]["arrangements_per_s"] * world,
+                "FT_arrangements_per_s": arr["fp64"]["FT"]["arrangements_per_s"] * world}
         if rates is not None and "fp64" in arr:
             # FP64 pipe model of the arrangement kernels: every (secondary node, primary
             # node) pair evaluates the reference's A (M) or B (F/T) fast node

@@ -396,7 +396,8 @@ class Coil:
                                                    compute_method=ComputeMethod.GPU,
                                                    precision_mode=PrecisionMode.FP64):
         """Coil::computeAllMutualInductanceArrangements (ComputeMInductanceMethods.cxx:200-260): (n,) array.
-        precision_mode FP32_COMPENSATED runs the primary quadrature in FP32 away from its winding."""
+        precision_mode FP32_COMPENSATED runs the primary quadrature in FP32 away from its winding;
+        FP32_REFINED also re-evaluates in FP64 the secondary nodes whose contributions dominate."""
         return Coil._arrangements(primary, secondary, primary_positions, secondary_positions, primary_y_angles,
                                   primary_z_angles, secondary_y_angles, secondary_z_angles,
                                   precision_factor or PrecisionFactor(), compute_method,

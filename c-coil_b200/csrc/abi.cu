@@ -501,6 +501,12 @@ int ccoil_set_point_ordering(int enabled)
 
 int ccoil_point_ordering(void) { return g_pointOrdering.load(); }
 
+}  // extern "C"
+
+double ccoil::refineFraction() { return g_refineFraction.load(); }
+
+extern "C" {
+
 int ccoil_set_refine_fraction(double fraction)
 {
     if (!(fraction >= 0.0) || !std::isfinite(fraction))

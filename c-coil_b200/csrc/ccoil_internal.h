@@ -191,6 +191,7 @@ constexpr size_t kNearPairBytes = 8;
 // benchmark group it re-evaluates about 12 % of the (point, coil) pairs in FP64
 // and brings the maximum relative error of A and B below 1e-7
 constexpr double kDefaultRefineFraction = 0.1;
+double refineFraction();  // the process-wide fraction (ccoil_set_refine_fraction)
 // FP32_REFINED evaluates the points in chunks whose stored contributions fit
 // this many bytes (the 128-coil benchmark group's A and B at 2^20 points take
 // 3.8 GB: one chunk), and lists at most kRefineListPairs pairs per chunk (8

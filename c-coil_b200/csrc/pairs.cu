@@ -23,6 +23,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -501,13 +502,23 @@ __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *t
 // memory and evaluates them with the FP64 integrands 32 at a time, so the FP64
 // work runs on full warps instead of dragging whole mixed iterations along;
 // the secondary-node sums and the cross-lane reduction stay FP64.
-template <int QTY, bool FP32>
+//
+// REFINE (FP32_REFINED, M and F/T): each secondary node's FP32 contribution is
+// also written to the warp's region of nodeScratch (node-major, W doubles per
+// node; deferred near-field nodes as zeros).  Once the warp has the primary's
+// total, every node whose contribution exceeds `fraction` of it (for F/T: of
+// the force or of the torque) is taken out of the sums and evaluated again
+// with the FP64 integrands, 32 at a time like the near-field nodes: the nodes
+// that dominate an arrangement whose ring sum cancels, whose FP32 errors the
+// cancellation magnifies.
+template <int QTY, bool FP32, bool REFINE = false>
 __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
                  const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
                  double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes,
                  const long long *__restrict__ zOffsets, long long *__restrict__ zList,
-                 unsigned long long *__restrict__ zListCount)
+                 unsigned long long *__restrict__ zListCount, double *__restrict__ nodeScratch, int scratchNodes,
+                 double fraction)
 {
     extern __shared__ __align__(16) unsigned char stagedPair[];
     __shared__ WarpPose warpPoses[4];
@@ -631,6 +642,8 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
             // of deferred nodes, in FP64, one per lane
             int nNear = 0;
             int *list = nearLists[threadIdx.x / 32];
+            // REFINE: this warp's node contributions
+            double *scr = REFINE ? nodeScratch + (size_t)warp * (size_t)scratchNodes * W : nullptr;
             auto node = [&](int n, bool valid, int mode) {
                 const int k = n % ph.s_na, lt_i = n / ph.s_na;
                 const int t = lt_i % ph.s_nt, l = lt_i / ph.s_nt;
@@ -659,6 +672,9 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         nNear += __popc(bal);
                         valid = valid && !near;
                     }
+                    if (REFINE && near)
+                        for (int i = 0; i < W; ++i)
+                            scr[(size_t)n * W + i] = 0.0;
                 }
                 if (QTY == 0)
                 {
@@ -672,8 +688,13 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     const double vx = -av * f.sphi, vy = av * f.cphi;
                     const double Ax = S.T[0] * vx + S.T[1] * vy, Ay = S.T[3] * vx + S.T[4] * vy,
                                  Az = S.T[6] * vx + S.T[7] * vy;
+                    const double c = (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
                     if (valid)
-                        part[0] += (Ax * tan[0] + Ay * tan[1] + Az * tan[2]) * w;
+                    {
+                        part[0] += c;
+                        if (REFINE && far)
+                            scr[n] = c;
+                    }
                 }
                 else if (QTY == 3)
                 {
@@ -810,8 +831,26 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         {
                             part[128 * i] += dF[i];
                             part[128 * (3 + i)] += dT[i];
+                            if (REFINE && far)
+                            {
+                                scr[(size_t)n * W + i] = dF[i];
+                                scr[(size_t)n * W + 3 + i] = dT[i];
+                            }
                         }
                 }
+            };
+            // 32 listed nodes (or the last few) in FP64
+            auto fp64Batch = [&]() {
+                __syncwarp();
+                const bool v = lane < nNear;
+                node(list[v ? lane : 0], v, 2);
+                const int rest = nNear > 32 ? nNear - 32 : 0;
+                const int moved = lane < rest ? list[32 + lane] : 0;
+                __syncwarp();
+                if (lane < rest)
+                    list[lane] = moved;
+                __syncwarp();
+                nNear = rest;
             };
             if (!FP32)
                 for (int n0 = 0; n0 < nsec; n0 += 32)
@@ -820,25 +859,59 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                 for (int n0 = 0; n0 < nsec || nNear > 0;)
                 {
                     if (nNear >= 32 || n0 >= nsec)
-                    {
-                        // 32 deferred near-field nodes (or the last few) in FP64
-                        __syncwarp();
-                        const bool v = lane < nNear;
-                        node(list[v ? lane : 0], v, 2);
-                        const int rest = nNear > 32 ? nNear - 32 : 0;
-                        const int moved = lane < rest ? list[32 + lane] : 0;
-                        __syncwarp();
-                        if (lane < rest)
-                            list[lane] = moved;
-                        __syncwarp();
-                        nNear = rest;
-                    }
+                        fp64Batch();  // deferred near-field nodes
                     else
                     {
                         node(n0 + lane < nsec ? n0 + lane : nsec - 1, n0 + lane < nsec, 1);
                         n0 += 32;
                     }
                 }
+            if (REFINE)
+            {
+                // the primary's totals (every lane), then the dominating nodes in FP64;
+                // node n was evaluated, and its contribution stored, by lane n % 32
+                double lim[2] = {0.0, 0.0};
+                for (int g = 0; g < (QTY == 0 ? 1 : 2); ++g)
+                {
+                    double n2 = 0.0;
+                    for (int i = 0; i < (QTY == 0 ? 1 : 3); ++i)
+                    {
+                        double v = part[128 * (3 * g + i)];
+#pragma unroll
+                        for (int off = 16; off > 0; off /= 2)
+                            v += __shfl_xor_sync(0xffffffffu, v, off);
+                        n2 += v * v;
+                    }
+                    lim[g] = fraction * fraction * n2;  // not finite: nothing is picked
+                }
+                for (int b0 = 0; b0 < nsec; b0 += 32)
+                {
+                    const int n = b0 + lane;
+                    bool pick = false;
+                    if (n < nsec)
+                    {
+                        double c[W];
+                        for (int i = 0; i < W; ++i)
+                            c[i] = scr[(size_t)n * W + i];
+                        if (QTY == 0)
+                            pick = c[0] * c[0] > lim[0];
+                        else
+                            pick = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] > lim[0] ||
+                                   c[3] * c[3] + c[4] * c[4] + c[5] * c[5] > lim[1];
+                        if (pick)
+                            for (int i = 0; i < W; ++i)
+                                part[128 * i] -= c[i];
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, pick);
+                    if (pick)
+                        list[nNear + __popc(bal & ((1u << lane) - 1u))] = n;
+                    nNear += __popc(bal);
+                    if (nNear >= 32)
+                        fp64Batch();
+                }
+                while (nNear > 0)
+                    fp64Batch();
+            }
             const double scale = QTY == 1 ? ph.f_factor : ph.m_factor;
 #pragma unroll
             for (int i = 0; i < W; ++i)
@@ -1080,12 +1153,17 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
     if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_PARAMETER_GRADIENT && count > 0 && (primary_count != 1 || !primary_poses))
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT,
                            "the parameter gradient needs exactly one primary with per-arrangement poses");
-    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED)
+    if (precision != CCOIL_PRECISION_FP64 && precision != CCOIL_PRECISION_FP32_COMPENSATED &&
+        precision != CCOIL_PRECISION_FP32_REFINED)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "unknown precision mode");
     if (precision == CCOIL_PRECISION_FP32_COMPENSATED && quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
         return failMessage(CCOIL_ERR_NOT_SUPPORTED,
                            "the position gradient is evaluated in FP64 only (the parameter gradient has an FP32 form)");
-    const bool fp32 = precision == CCOIL_PRECISION_FP32_COMPENSATED;
+    if (precision == CCOIL_PRECISION_FP32_REFINED && quantity != CCOIL_PAIR_MUTUAL_INDUCTANCE &&
+        quantity != CCOIL_PAIR_FORCE_TORQUE)
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "FP32_REFINED covers mutual inductance and force/torque");
+    const bool fp32 = precision != CCOIL_PRECISION_FP64;
+    const bool refine = precision == CCOIL_PRECISION_FP32_REFINED;
     if (memory != CCOIL_MEMORY_HOST && memory != CCOIL_MEMORY_DEVICE)
         return failMessage(CCOIL_ERR_INVALID_ARGUMENT, "memory must be HOST or DEVICE");
     if (z_axis_count)
@@ -1127,7 +1205,7 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
             if (!buildZAxis(primaries[j], *secondary, zaxis_precisions[2 * j], zaxis_precisions[2 * j + 1], blob, err))
                 return fail(CCOIL_ERR_INVALID_ARGUMENT, "primary " + std::to_string(j) + ": " + err);
         }
-    DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ, dZOff, dZList, dZCount;
+    DevBuf dBlob, dOff, dPrim, dSec, dOut, dZ, dZOff, dZList, dZCount, dScratch;
     cudaError_t e = dBlob.alloc(blob.size(), st);
     if (e == cudaSuccess)
         e = dOff.alloc(sizeof(long long) * offsets.size(), st);
@@ -1184,6 +1262,22 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
     long long blocks = (warpsNeeded + 3) / 4;
     if (blocks > 148LL * 64)
         blocks = 148LL * 64;
+    // FP32_REFINED: every warp's region of node contributions (the grid strides over
+    // the arrangements, so the scratch is sized by the grid, not by the count)
+    int scratchNodes = 0;
+    if (refine)
+    {
+        for (long long off : offsets)
+        {
+            const PairHeader *ph = reinterpret_cast<const PairHeader *>(blob.data() + off);
+            scratchNodes = std::max(scratchNodes, ph->s_nl * ph->s_nt * ph->s_na);
+        }
+        e = dScratch.alloc(sizeof(double) * (size_t)width * (size_t)scratchNodes * (size_t)blocks * 4, st);
+        if (e != cudaSuccess)
+            return cudaFail(e, "refinement scratch");
+    }
+    const double fraction = refineFraction();
+    auto *scratch = static_cast<double *>(dScratch.p);
     auto *zc = static_cast<unsigned long long *>(dZ.p);
     const auto *dB = static_cast<const unsigned char *>(dBlob.p);
     const auto *dO = static_cast<const long long *>(dOff.p);
@@ -1191,15 +1285,19 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
     const auto *zO = static_cast<const long long *>(dZOff.p);
     auto *zL = static_cast<long long *>(dZList.p);
     auto *zN = static_cast<unsigned long long *>(dZCount.p);
-#define CCOIL_PAIR_LAUNCH(Q, F)                                                                                        \
-    pairKernel64<Q, F><<<(unsigned)blocks, 128, smem, st>>>(dB, dO, primary_count, primP, secP, count, o, zc,       \
-                                                           stagedBytes, zO, zL, zN)
+#define CCOIL_PAIR_LAUNCH(Q, F, ...)                                                                                   \
+    pairKernel64<Q, F, ##__VA_ARGS__><<<(unsigned)blocks, 128, smem, st>>>(                                          \
+        dB, dO, primary_count, primP, secP, count, o, zc, stagedBytes, zO, zL, zN, scratch, scratchNodes, fraction)
     if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE && !fp32)
         CCOIL_PAIR_LAUNCH(0, false);
+    else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE && refine)
+        CCOIL_PAIR_LAUNCH(0, true, true);
     else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE)
         CCOIL_PAIR_LAUNCH(0, true);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE && !fp32)
         CCOIL_PAIR_LAUNCH(1, false);
+    else if (quantity == CCOIL_PAIR_FORCE_TORQUE && refine)
+        CCOIL_PAIR_LAUNCH(1, true, true);
     else if (quantity == CCOIL_PAIR_FORCE_TORQUE)
         CCOIL_PAIR_LAUNCH(1, true);
     else if (quantity == CCOIL_PAIR_MUTUAL_INDUCTANCE_GRADIENT)
