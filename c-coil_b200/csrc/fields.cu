@@ -280,7 +280,7 @@ cudaError_t launchField(const FieldLaunch &L, cudaStream_t st)
     refineSelectKernel<W><<<(unsigned)selectBlocks, 256, 0, st>>>(L.d_out, L.d_contrib, L.npts, L.nseg,
                                                                   L.refine_fraction, L.d_refine_segs, work,
                                                                   L.work_capacity);
-    refinePairsKernel64<FIELD><<<148 * CCOIL_FP64_MIN_BLOCKS, 128, 0, st>>>(L.d_blob, L.d_segs, L.d_points, L.d_out,
+    refinePairsKernel64<FIELD><<<148 * refineMinBlocks(FIELD), 128, 0, st>>>(L.d_blob, L.d_segs, L.d_points, L.d_out,
                                                                            work, L.work_capacity, L.d_work_count);
     return cudaGetLastError();
 }

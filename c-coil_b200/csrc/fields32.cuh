@@ -293,8 +293,18 @@ __global__ void __launch_bounds__(256) nearFieldKernel(const unsigned char *__re
 // (FP64 atomics).  Consecutive list entries mostly share their segment (the
 // selection lists a warp's picks of one segment together), so the lanes of a
 // warp run loops of the same length.  Grid-stride over the device-side count.
+// CTAs per SM of the FP64 pair pass: the most at which each field's FP64
+// integrands compile without spills (vector potential 78 registers, field 96,
+// gradient 122)
+#ifndef CCOIL_REFINE_MIN_BLOCKS_B
+#define CCOIL_REFINE_MIN_BLOCKS_B 5
+#endif
+constexpr int refineMinBlocks(int field)
+{
+    return field == CCOIL_FIELD_B ? CCOIL_REFINE_MIN_BLOCKS_B : (field == CCOIL_FIELD_G ? 4 : 6);
+}
 template <int FIELD>
-__global__ void __launch_bounds__(128, CCOIL_FP64_MIN_BLOCKS) refinePairsKernel64(
+__global__ void __launch_bounds__(128, refineMinBlocks(FIELD)) refinePairsKernel64(
     const unsigned char *__restrict__ blob, const SegmentDesc *__restrict__ segs, const double *__restrict__ points,
     double *__restrict__ out, const NearPair *__restrict__ work, unsigned long long workCapacity,
     const unsigned long long *__restrict__ workCount)
