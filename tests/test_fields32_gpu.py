@@ -189,7 +189,12 @@ def test_mirror_pair_tables(ccoil, angular):
 def test_refined_mode(ccoil):
     """FP32_REFINED replaces by its FP64 value every (point, coil) contribution whose
     norm exceeds the set fraction of the point's total.  With fraction 0 every pair
-    is FP64 and the result is the FP64 path's up to summation order; at the default
+    is FP64: the field and the gradient are the FP64 path's up to summation order
+    (the field's reciprocal square roots come from Newton steps: 1e-14); the vector
+    potential (and E) takes a cancellation-free FP64 form in the refinement pass,
+    which differs from the FP64 path's operation sequence (the reference's, whose
+    own cancellation errors reach ~2e-10 on single pairs) by at most 1e-9, median
+    below 1e-13; at the default
     0.1 the maximum error of A, B and E falls below 1e-7 on the 16-coil group
     (from the FP32 path's 4-6e-7), with part of the pairs refined; the gradient
     stays within its FP32 bars.  Fractions must be finite and
@@ -213,7 +218,10 @@ def test_refined_mode(ccoil):
             n_all = plan.refined_pairs()
             plan.close()
             assert 0.9 * len(pts) * len(coils) <= n_all <= len(pts) * len(coils), (field, n_all)
-            assert rel_err(got, f64).max() < 1e-13, (field, rel_err(got, f64).max())
+            e0 = rel_err(got, f64)
+            print(field, "fraction 0: median %.1e max %.1e" % (np.median(e0), e0.max()))
+            bar0 = {0: 1e-9, 1: 1e-13, 2: 1e-9, 3: 1e-13}[field]
+            assert np.median(e0) < 1e-13 and e0.max() < bar0, (field, np.median(e0), e0.max())
             L.ccoil_set_refine_fraction(ctypes.c_double(default))
             plan = ccoil.FieldPlan([c.struct() for c in coils], field, ccoil.PrecisionMode.FP32_REFINED)
             got = plan(pts)
