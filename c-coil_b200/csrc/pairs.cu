@@ -421,6 +421,9 @@ __device__ __forceinline__ void transformDerivatives(double yA, double zA, doubl
 #ifndef CCOIL_PAIR32_MIN_BLOCKS
 #define CCOIL_PAIR32_MIN_BLOCKS 9
 #endif
+// FP32_REFINED arrangements: the largest scratch of node contributions (the
+// grid shrinks to fit it)
+constexpr size_t kPairRefineScratchBytes = size_t(1) << 30;
 // largest single-primary blob staged in shared memory (0 turns staging off)
 #ifndef CCOIL_PAIR_STAGE_MAX_BYTES
 #define CCOIL_PAIR_STAGE_MAX_BYTES (48 * 1024)
@@ -1272,7 +1275,12 @@ int ccoil::pairArrangements(const ccoil_coil_t *primaries, int primary_count, co
             const PairHeader *ph = reinterpret_cast<const PairHeader *>(blob.data() + off);
             scratchNodes = std::max(scratchNodes, ph->s_nl * ph->s_nt * ph->s_na);
         }
-        e = dScratch.alloc(sizeof(double) * (size_t)width * (size_t)scratchNodes * (size_t)blocks * 4, st);
+        // at most kPairRefineScratchBytes: a secondary with many nodes runs on fewer
+        // warps (each keeps 1 or 6 doubles per node), never fewer than one CTA per SM
+        const size_t perBlock = sizeof(double) * (size_t)width * (size_t)scratchNodes * 4;
+        const long long fit = (long long)(kPairRefineScratchBytes / perBlock);
+        blocks = std::max(1LL, std::min(blocks, std::max(fit, 148LL)));
+        e = dScratch.alloc(perBlock * (size_t)blocks, st);
         if (e != cudaSuccess)
             return cudaFail(e, "refinement scratch");
     }

@@ -49,11 +49,13 @@ typedef enum ccoil_status
 /* Arithmetic of the quadrature.  FP64 reproduces the reference's double CPU
  * path; FP32_COMPENSATED runs the bulk of the nodes in FP32 with compensated
  * accumulation and keeps FP64 for near-field points and the final sums;
- * FP32_REFINED (field plans) is FP32_COMPENSATED in which every (point, coil)
- * contribution whose norm exceeds a set fraction of the norm of the point's
- * total is replaced by its FP64 value (ccoil_set_refine_fraction): where the
- * coils' fields cancel, the contributions that dominate carry errors that the
- * cancellation magnifies, and those are re-evaluated. */
+ * FP32_REFINED (field plans, and mutual inductance and force/torque
+ * arrangements) is FP32_COMPENSATED in which every (point, coil) contribution
+ * (arrangements: every secondary node's contribution) whose norm exceeds a set
+ * fraction of the norm of the total is replaced by its FP64 value
+ * (ccoil_set_refine_fraction): where the contributions cancel, those that
+ * dominate carry errors that the cancellation magnifies, and those are
+ * re-evaluated. */
 typedef enum ccoil_precision
 {
     CCOIL_PRECISION_FP64 = 0,
@@ -258,7 +260,11 @@ typedef struct ccoil_pose
  * evaluates the primary's quadrature
  * in FP32 with compensated sums, except where a secondary node lies within the
  * primary's near-field box (winding cross-section inflated by 0.1 R), which
- * is evaluated in FP64; sums over secondary nodes and primaries are FP64. */
+ * is evaluated in FP64; sums over secondary nodes and primaries are FP64.
+ * CCOIL_PRECISION_FP32_REFINED (mutual inductance and force/torque) also
+ * re-evaluates in FP64 every secondary node whose contribution exceeds the
+ * refinement fraction of the arrangement's M (of its force or of its torque);
+ * it keeps each warp's node contributions in up to 1 GiB of device scratch. */
 int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
                             const ccoil_precision_args_t *secondary_precisions, const ccoil_pose_t *primary_poses,
                             const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
