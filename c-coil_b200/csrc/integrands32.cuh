@@ -135,7 +135,8 @@ struct PlainSum
 
 // FP64 running sum: each entry's two pair terms are added in FP32 (one
 // rounding, relative to that entry's own term), converted and added in FP64,
-// on the FP64 pipe, which the FP32 integrands leave idle
+// on pipes the FP32 integrands leave idle (the conversion built from the
+// IEEE fields on the integer pipe instead measured 7 % slower for B)
 struct F64Sum
 {
     double s = 0.0;
