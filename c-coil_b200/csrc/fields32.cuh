@@ -16,6 +16,7 @@
 // near-field kernel adds those pairs back evaluated with the FP64 integrands.
 
 #include "integrands32.cuh"
+#include "integrands64f.cuh"
 
 // Integrates one segment for one lane and adds the lane's contribution to acc.
 template <int FIELD, int LANES>
@@ -286,164 +287,6 @@ __global__ void __launch_bounds__(256) nearFieldKernel(const unsigned char *__re
     }
 }
 
-// FP64 arithmetic of the refinement pass.  The pass needs FP64 accuracy, not
-// the reference's operation sequence (which the FP64 field kernels keep for
-// 1e-12 parity), so it takes cheaper forms of the same quantities:
-//   rsqrt64: 1/sqrt(x) from the FP32 MUFU estimate (relative error below
-//            2^-22.9) and two Newton-Raphson steps y <- y + y (1 - x y^2) / 2,
-//            each squaring the relative error (below 2^-45, then below FP64's
-//            rounding); arguments outside FP32's normal range take the IEEE path
-//   sqrt64:  x rsqrt64(x)
-__device__ __forceinline__ double rsqrt64(double x)
-{
-    if (!(x > 1e-36 && x < 1e36))
-        return 1.0 / sqrt(x);
-    double y = (double)rsqrtNR((float)x);
-    double e = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, e, y);
-    e = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, e, y);
-}
-__device__ __forceinline__ double sqrt64(double x) { return x * rsqrt64(x); }
-
-// The vector potential of one segment at one point, one thread, for the
-// refinement pass.  Fast method: the reference's node value is
-// log((e1 + d1) / (e2 + d2)) = asinh(top / sqrt(D)) - asinh(bot / sqrt(D))
-// (D = p^2 + r^2 - 2 p r c, e = sqrt(d^2 + 1)).  With A1 = |top| + s1,
-// A2 = |bot| + s2, s = sqrt(top^2 + D) or sqrt(bot^2 + D), it is
-// log(A1 / A2) above the coil's length slab (bot >= 0), log(A2 / A1) below it
-// (top < 0) and log(A1 A2 / D) inside it: log(num / den) with num and den
-// products of positive terms, so nothing cancels (the reference's e + d for
-// d << 0 does), and two square roots per node instead of three.  The FP32-mode
-// table holds the nodes as mirror pairs (phi, pi - phi) whose weighted cosines
-// are opposite (symmetric Gauss-Legendre nodes and weights, up to their
-// rounding), so a pair takes one logarithm:
-//   w c lg + w' c' lg' = ((w c - w' c') / 2) log(num den' / (den num')).
-// Against 40-digit arithmetic a pair is within 1.1e-11 (relative) where the
-// reference's sequence is off by up to 2e-10.
-// Slow method: w c p / sqrt(D) per node, as the reference.
-__device__ __forceinline__ double segmentA64Refine(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                                   const double2 *pt, const Frame &f)
-{
-    double sum = 0.0;
-    const int n = h.n_phi;
-    if (h.fast)
-    {
-        const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r;
-            const double T2 = top * top, B2 = bot * bot, aT = fabs(top), aB = fabs(bot);
-            const bool above = bot >= 0.0, below = top < 0.0;
-            auto ratio = [&](double c, double &num, double &den) {
-                const double D = cB - cA * c;
-                const double a1 = aT + sqrt64(T2 + D), a2 = aB + sqrt64(B2 + D);
-                num = above ? a1 : (below ? a2 : a1 * a2);
-                den = above ? a2 : (below ? a1 : D);
-            };
-            double part = 0.0;
-            int k = 0;
-            for (; k + 1 < n; k += 2)
-            {
-                const double2 q = pt[k], qm = pt[k + 1];
-                double n1, e1, n2, e2;
-                ratio(q.x, n1, e1);
-                ratio(qm.x, n2, e2);
-                part += 0.5 * (q.y * q.x - qm.y * qm.x) * log64((n1 * e2) / (e1 * n2));
-            }
-            if (k < n)
-            {
-                // an odd table's middle node
-                const double2 q = pt[k];
-                double n1, e1;
-                ratio(q.x, n1, e1);
-                part += q.y * q.x * log64(n1 / e1);
-            }
-            sum += t.y * t.x * part;
-        }
-    }
-    else
-    {
-        for (int i = 0; i < h.n_l; ++i)
-        {
-            const double2 l = lt[i];
-            const double zl = l.x + f.z;
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r + zl * zl;
-                double part = 0.0;
-                for (int k = 0; k < n; ++k)
-                {
-                    const double2 q = pt[k];
-                    part += q.y * q.x * rsqrt64(cB - cA * q.x);
-                }
-                sum += l.y * t.y * t.x * part;
-            }
-        }
-    }
-    return sum;
-}
-
-// The field of one segment at one point, one thread, for the refinement pass:
-// the reference's node values with every 1/sqrt(D) from rsqrt64 (fast method:
-// w c (g2 - g1) and w (p^2 - p r c) / rho^2 (top g1 - bot g2); slow method:
-// w g^3 (p^2 - p r c) and w g^3 p zl c)
-__device__ __forceinline__ void segmentB64Refine(const SegmentHeader &h, const double2 *tt, const double2 *lt,
-                                                 const double2 *pt, const Frame &f, double &H, double &Z)
-{
-    H = 0.0;
-    Z = 0.0;
-    if (h.fast)
-    {
-        const double top = f.z + h.half_length, bot = f.z - h.half_length;
-        for (int j = 0; j < h.n_t; ++j)
-        {
-            const double2 t = tt[j];
-            const double cA = t.x * t.x, cB = t.x * f.r, cC = cA + f.r * f.r;
-            const double d1 = top * top + cC, d2 = bot * bot + cC;
-            double h0 = 0.0, z0 = 0.0;
-            for (int k = 0; k < h.n_phi; ++k)
-            {
-                const double2 q = pt[k];
-                const double F = 2.0 * cB * q.x;
-                const double g1 = rsqrt64(d1 - F), g2 = rsqrt64(d2 - F);
-                h0 += q.y * q.x * (g2 - g1);
-                z0 += q.y * ((cA - 0.5 * F) / (cC - F)) * (top * g1 - bot * g2);
-            }
-            H += t.y * t.x * h0;
-            Z += t.y * z0;
-        }
-    }
-    else
-    {
-        for (int i = 0; i < h.n_l; ++i)
-        {
-            const double2 l = lt[i];
-            const double zl = l.x + f.z;
-            for (int j = 0; j < h.n_t; ++j)
-            {
-                const double2 t = tt[j];
-                const double cA = t.x * t.x, cB = t.x * zl, cC = t.x * f.r;
-                const double cD = cA + f.r * f.r + zl * zl;
-                double h0 = 0.0, z0 = 0.0;
-                for (int k = 0; k < h.n_phi; ++k)
-                {
-                    const double2 q = pt[k];
-                    const double g = rsqrt64(cD - 2.0 * cC * q.x);
-                    const double wg3 = q.y * (g * g * g);
-                    z0 += wg3 * (cA - cC * q.x);
-                    h0 += wg3 * (cB * q.x);
-                }
-                const double w = l.y * t.y;
-                H += w * h0;
-                Z += w * z0;
-            }
-        }
-    }
-}
-
 // One segment at one point for the refinement pass: the vector potential (and
 // E) and the field with the forms above, the gradient with the FP64 field
 // integrands
@@ -464,12 +307,12 @@ __device__ __forceinline__ void integrateSegmentRefine(const unsigned char *seg,
     if (FIELD == CCOIL_FIELD_B)
     {
         double H, Z;
-        segmentB64Refine(h, tt, lt, pt, f, H, Z);
+        segmentB64Fast(h, tt, lt, pt, f, H, Z);
         addRotated(h, H * f.cphi, H * f.sphi, Z, acc);
     }
     else
     {
-        const double a = segmentA64Refine(h, tt, lt, pt, f) * h.field_factor;
+        const double a = segmentA64Fast<true>(h, tt, lt, pt, f) * h.field_factor;
         addRotated(h, -a * f.sphi, a * f.cphi, 0.0, acc);
     }
 }

@@ -35,6 +35,7 @@ namespace
 {
 #include "integrands64.cuh"
 #include "integrands32.cuh"
+#include "integrands64f.cuh"
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kMuReduced = 1e-7;
@@ -471,6 +472,23 @@ __device__ __noinline__ double2 pairB64(const SegmentHeader &h, const double2 *t
     return make_double2(H, Z);
 }
 
+// The FP32 kernels' FP64 nodes (near-field and refined): FP64 accuracy without
+// the reference's operation sequence, in the cheaper forms of
+// integrands64f.cuh (the table is in the reference's order)
+__device__ __noinline__ double pairA64Fast(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                           const double2 *pt, double z, double r)
+{
+    return segmentA64Fast<false>(h, tt, lt, pt, frameZR(z, r));
+}
+
+__device__ __noinline__ double2 pairB64Fast(const SegmentHeader &h, const double2 *tt, const double2 *lt,
+                                            const double2 *pt, double z, double r)
+{
+    double H, Z;
+    segmentB64Fast(h, tt, lt, pt, frameZR(z, r), H, Z);
+    return make_double2(H, Z);
+}
+
 // The FP32 primary quadrature, out of line as well: the loop over the
 // primary's nodes gets the whole register budget.  Its pair sums are plain
 // FP32: the FP64 sum over the secondary's nodes averages their rounding
@@ -687,7 +705,7 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                     else if (far)
                         av = pairA32(h, tt, lt, pn, f.z, f.r);
                     else
-                        av = pairA64(h, tt, lt, pt, f.z, f.r);
+                        av = pairA64Fast(h, tt, lt, pt, f.z, f.r);
                     const double vx = -av * f.sphi, vy = av * f.cphi;
                     const double Ax = S.T[0] * vx + S.T[1] * vy, Ay = S.T[3] * vx + S.T[4] * vy,
                                  Az = S.T[6] * vx + S.T[7] * vy;
@@ -816,7 +834,9 @@ __global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PA
                         segmentB64<1>(h, tt, lt, pt, f, 0, H, Z);
                     else
                     {
-                        const double2 hz = FP32 && far ? pairB32(h, tt, lt, pn, f.z, f.r) : pairB64(h, tt, lt, pt, f.z, f.r);
+                        const double2 hz = !FP32 ? pairB64(h, tt, lt, pt, f.z, f.r)
+                                                 : far ? pairB32(h, tt, lt, pn, f.z, f.r)
+                                                       : pairB64Fast(h, tt, lt, pt, f.z, f.r);
                         H = hz.x;
                         Z = hz.y;
                     }
