@@ -103,3 +103,16 @@ def gradient_band(rows, pts, widen=0.1):
         R, a = row[0], row[1]
         band |= (r > R - widen * R) & (r < R + a + widen * R)
     return band
+
+
+def winding_near(rows, pts, margin=0.1):
+    """Points inside any coil's winding cross-section box in its (r, z) frame,
+    inflated by margin*R: the near field, where the FP32 paths evaluate in FP64 and
+    the FP32 error statistics are taken away from."""
+    rows = np.atleast_2d(rows)
+    near = np.zeros(len(pts), dtype=bool)
+    for row in rows:
+        r, z = coil_frame(row, pts)
+        R, a, b = row[0], row[1], row[2]
+        near |= (r > R - margin * R) & (r < R + a + margin * R) & (np.abs(z) < 0.5 * b + margin * R)
+    return near

@@ -301,3 +301,23 @@ def test_point_ordering(ccoil):
             assert rel_err(on[good], off[good]).max() < 2e-6, field
     finally:
         L.ccoil_set_point_ordering(1)
+
+
+def test_refined_group128_below_1e7(ccoil):
+    """The bench's 128-coil group (PF 5) on 2^18 points of another seed: FP32_REFINED at
+    its default fraction keeps A, B and E within 1e-7 of FP64 away from windings,
+    where FP32_COMPENSATED reaches 1e-6 and more."""
+    import torch
+    from ccoil_b200 import workloads
+    from conftest import winding_near
+    rows, _ = workloads.group_config(coils=128, points=1)
+    coils = workloads.coils_from_rows(rows, 5.0)
+    pts = workloads.points_cube(1 << 18, seed=4242)
+    away = ~winding_near(rows, pts)
+    for field in (0, 1, 2):
+        f64 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP64)
+        f32 = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_COMPENSATED)
+        ref = evaluate(ccoil, coils, pts, field, ccoil.PrecisionMode.FP32_REFINED)
+        e, e32 = rel_err(ref, f64)[away], rel_err(f32, f64)[away]
+        print(field, "refined max %.1e p99 %.1e (FP32c max %.1e)" % (e.max(), np.quantile(e, 0.99), e32.max()))
+        assert e.max() < 1e-7, (field, e.max())
