@@ -103,7 +103,10 @@ cudaError_t scratchAlloc(void **p, size_t bytes, cudaStream_t st)
                 g_pools[dev] = nullptr;
                 return e;
             }
-            unsigned long long keep = 1ULL << 32;
+            // freed blocks up to 16 GiB stay mapped for the next allocation: a
+            // one-shot FP32_REFINED call frees and takes again ~5 GB of scratch
+            // (with 4 GiB kept, the remapping made those calls 1.5x slower)
+            unsigned long long keep = 1ULL << 34;
             e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
             if (e != cudaSuccess)
                 return e;
