@@ -367,9 +367,12 @@ int ccoil_inject_allocation_failures(int count);
  * inside a host program that owns every device allocation (and budgets the
  * device memory itself), real-time loops that must not stall on an
  * allocation.
- * Same arguments and results as ccoil_compute_fields with precision
- * FP32_COMPENSATED, except that `points` and `out` must be device pointers
- * and the call is asynchronous on `stream`.
+ * Same arguments as ccoil_compute_fields with precision FP32_COMPENSATED,
+ * except that `points` and `out` must be device pointers and the call is
+ * asynchronous on `stream`; the same results up to 16,383 points (from 16,384
+ * on, ccoil_compute_fields evaluates the points in Morton order, see
+ * ccoil_set_point_ordering, and the two differ by FP32 rounding; this entry
+ * point keeps the caller's order).
  *
  * Its scratch (node tables, segment list, near-field work list) is one fixed
  * 3 MiB array in device memory, held by every GPU that loads the library until
