@@ -8,7 +8,7 @@ PrecisionArguments.  Seeded synthetic data; no dataset is involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32c|fp32r|both|all]
     python bench.py --impl reference        # the reference's own CPU_MT code on this host
-    python bench.py --workload refine-sweep # FP32_REFINED's cost and error over its fraction
+    python bench.py --workload refine-sweep # FP32_REFINED: cost and error over its fraction (fields, arrangements)
 
 The headline configuration (fp32r) is the FP32 one whose maximum error away
 from windings stays below 1e-7: FP32_REFINED for A and B, FP32_COMPENSATED
@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--workload", default="group", choices=["group", "batched", "adjoint", "pf-sweep", "refine-sweep"],
                     help="group: the headline coil-group fields + pair arrangements; batched: many independent "
                          "systems in one persistent launch; adjoint: forward + backward of the B-field loss; "
-                         "pf-sweep: the group at PrecisionFactor 1, 3, 5, 7, 9 (2^18 points)")
+                         "pf-sweep: the group at PrecisionFactor 1, 3, 5, 7, 9 (2^18 points); refine-sweep: "
+                         "FP32_REFINED's time and error per fraction, fields and pair arrangements")
     ap.add_argument("--systems", type=int, default=2048, help="independent systems of the batched workload")
     return ap.parse_args()
 
@@ -533,8 +534,59 @@ def bench_refine_sweep(a):
         res["fp32c"]["speedup_vs_fp64"] = res["fp64"]["ms"] / res["fp32c"]["ms"]
         curve[name] = res
     L.ccoil_set_refine_fraction(ctypes.c_double(default_fraction))
+    pair_curve = refine_sweep_arrangements(a, cc, workloads, dev, L, default_fraction) if a.arrangements > 0 else None
     print(json.dumps({"workload": "refine-sweep", "default_fraction": default_fraction, "config": workload_config(a, 1),
-                      "steps": a.steps, "coils": a.coils, "l2": "flushed between timed evaluations", "curve": curve}))
+                      "steps": a.steps, "coils": a.coils, "l2": "flushed between timed evaluations", "curve": curve,
+                      "arrangements": pair_curve}))
+
+
+def refine_sweep_arrangements(a, cc, workloads, dev, L, default_fraction):
+    """The same curve for the pair arrangements: M and F/T in FP64, FP32_COMPENSATED
+    and FP32_REFINED at each fraction, time and error against FP64 over all
+    arrangements (F and T separately)."""
+    import ctypes
+    import torch
+    from ccoil_b200.coil import pair_arrangements_device
+    _, _, pstruct, sstruct, spre, pposes, sposes, _ = pair_setup(cc, workloads, a.arrangements, 3)
+    dp = torch.from_numpy(pposes).to(dev)
+    ds = torch.from_numpy(sposes).to(dev)
+    fractions = [0.1, 0.03, 0.01, 0.005, 0.003]
+
+    def timed(q, w, mode):
+        out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
+        for _ in range(max(a.warmup, 1)):
+            pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out, precision_mode=mode)
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pair_arrangements_device([pstruct], sstruct, [spre], dp, ds, q, out, precision_mode=mode)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / a.steps, out
+
+    def errors(name, got, ref):
+        if name == "M":
+            return {"M": rel_err_stats(got, ref)}
+        return {"F": rel_err_stats(got[:, :3], ref[:, :3]), "T": rel_err_stats(got[:, 3:], ref[:, 3:])}
+
+    curve = {}
+    try:
+        for name, q, w in (("M", 0, 1), ("FT", 1, 6)):
+            ms64, ref = timed(q, w, cc.PrecisionMode.FP64)
+            res = {"fp64": {"ms": ms64}}
+            ms, out = timed(q, w, cc.PrecisionMode.FP32_COMPENSATED)
+            res["fp32c"] = {"ms": ms, "speedup_vs_fp64": ms64 / ms, "err": errors(name, out, ref)}
+            for fr in fractions:
+                L.ccoil_set_refine_fraction(ctypes.c_double(fr))
+                ms, out = timed(q, w, cc.PrecisionMode.FP32_REFINED)
+                res["fraction_%g" % fr] = {"ms": ms, "speedup_vs_fp64": ms64 / ms, "err": errors(name, out, ref)}
+            curve[name] = res
+    finally:
+        L.ccoil_set_refine_fraction(ctypes.c_double(default_fraction))
+    return {"count": a.arrangements, "curve": curve}
 
 
 def main():
