@@ -1,29 +1,15 @@
 #ifndef CCOIL_INTEGRANDS64F_CUH
 #define CCOIL_INTEGRANDS64F_CUH
 
+#include "fp64ops.cuh"
+
 // Cheaper FP64 forms of the vector potential and the field, for FP64 work that
 // needs FP64 accuracy but not the reference's operation sequence (which the
 // FP64 field and arrangement kernels keep for 1e-12 parity): the refinement
 // pass of FP32_REFINED plans, and the FP64 nodes (near-field and refined) of
 // the FP32 arrangement kernels.  Included inside the kernels' anonymous
-// namespaces after integrands64.cuh and integrands32.cuh.
-//
-//   rsqrt64: 1/sqrt(x) from the FP32 MUFU estimate (relative error below
-//            2^-22.9) and two Newton-Raphson steps y <- y + y (1 - x y^2) / 2,
-//            each squaring the relative error (below 2^-45, then below FP64's
-//            rounding); arguments outside FP32's normal range take the IEEE path
-//   sqrt64:  x rsqrt64(x)
-__device__ __forceinline__ double rsqrt64(double x)
-{
-    if (!(x > 1e-36 && x < 1e36))
-        return 1.0 / sqrt(x);
-    double y = (double)rsqrtNR((float)x);
-    double e = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, e, y);
-    e = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, e, y);
-}
-__device__ __forceinline__ double sqrt64(double x) { return x * rsqrt64(x); }
+// namespaces after integrands64.cuh; the reciprocal square roots, square roots
+// and divisions come from fp64ops.cuh.
 
 // The vector potential of one segment at one point, one thread.  Fast method:
 // the reference's node value is log((e1 + d1) / (e2 + d2)) =
@@ -43,6 +29,37 @@ __device__ __forceinline__ double sqrt64(double x) { return x * rsqrt64(x); }
 // Against 40-digit arithmetic a pair is within 1.1e-11 (relative) where the
 // reference's sequence is off by up to 2e-10.
 // Slow method: w c p / sqrt(D) per node, as the reference.
+// One thickness node of the fast method: sum over the angular nodes.
+template <bool PAIRED, bool CHECKED>
+__device__ __forceinline__ double phiLoopA64(const double2 *pt, int n, double cA, double cB, double T2, double B2,
+                                             double aT, double aB, bool above, bool below)
+{
+    auto ratio = [&](double c, double &num, double &den) {
+        const double D = cB - cA * c;
+        const double a1 = aT + sqrt64t<CHECKED>(T2 + D), a2 = aB + sqrt64t<CHECKED>(B2 + D);
+        num = above ? a1 : (below ? a2 : a1 * a2);
+        den = above ? a2 : (below ? a1 : D);
+    };
+    double part = 0.0;
+    for (int m = 0; m < n / 2; ++m)
+    {
+        const double2 q = pt[PAIRED ? 2 * m : m], qm = pt[PAIRED ? 2 * m + 1 : n - 1 - m];
+        double n1, e1, n2, e2;
+        ratio(q.x, n1, e1);
+        ratio(qm.x, n2, e2);
+        part += 0.5 * (q.y * q.x - qm.y * qm.x) * log64(div64t<CHECKED>(n1 * e2, e1 * n2));
+    }
+    if (n & 1)
+    {
+        // an odd table's middle node
+        const double2 q = pt[PAIRED ? n - 1 : n / 2];
+        double n1, e1;
+        ratio(q.x, n1, e1);
+        part += q.y * q.x * log64(div64t<CHECKED>(n1, e1));
+    }
+    return part;
+}
+
 template <bool PAIRED>
 __device__ __forceinline__ double segmentA64Fast(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                                    const double2 *pt, const Frame &f)
@@ -52,35 +69,20 @@ __device__ __forceinline__ double segmentA64Fast(const SegmentHeader &h, const d
     if (h.fast)
     {
         const double top = f.z + h.half_length, bot = f.z - h.half_length;
+        const double T2 = top * top, B2 = bot * bot, aT = fabs(top), aB = fabs(bot);
+        const bool above = bot >= 0.0, below = top < 0.0;
         for (int j = 0; j < h.n_t; ++j)
         {
             const double2 t = tt[j];
             const double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r;
-            const double T2 = top * top, B2 = bot * bot, aT = fabs(top), aB = fabs(bot);
-            const bool above = bot >= 0.0, below = top < 0.0;
-            auto ratio = [&](double c, double &num, double &den) {
-                const double D = cB - cA * c;
-                const double a1 = aT + sqrt64(T2 + D), a2 = aB + sqrt64(B2 + D);
-                num = above ? a1 : (below ? a2 : a1 * a2);
-                den = above ? a2 : (below ? a1 : D);
-            };
-            double part = 0.0;
-            for (int m = 0; m < n / 2; ++m)
-            {
-                const double2 q = pt[PAIRED ? 2 * m : m], qm = pt[PAIRED ? 2 * m + 1 : n - 1 - m];
-                double n1, e1, n2, e2;
-                ratio(q.x, n1, e1);
-                ratio(qm.x, n2, e2);
-                part += 0.5 * (q.y * q.x - qm.y * qm.x) * log64((n1 * e2) / (e1 * n2));
-            }
-            if (n & 1)
-            {
-                // an odd table's middle node
-                const double2 q = pt[PAIRED ? n - 1 : n / 2];
-                double n1, e1;
-                ratio(q.x, n1, e1);
-                part += q.y * q.x * log64(n1 / e1);
-            }
+            // D in [cB - |cA|, cB + |cA|], the roots' arguments T2 + D and B2 + D
+            // above it; D (the divisor inside the slab) and the products of
+            // a = |t| + sqrt(t^2 + D) >= sqrt(D) that reach the division stay in
+            // FP64's normal range with them
+            const double k = fabs(cA);
+            const bool fast = inRange64(cB - k, fmax(T2, B2) + (cB + k));
+            const double part = fast ? phiLoopA64<PAIRED, false>(pt, n, cA, cB, T2, B2, aT, aB, above, below)
+                                     : phiLoopA64<PAIRED, true>(pt, n, cA, cB, T2, B2, aT, aB, above, below);
             sum += t.y * t.x * part;
         }
     }
@@ -95,11 +97,18 @@ __device__ __forceinline__ double segmentA64Fast(const SegmentHeader &h, const d
                 const double2 t = tt[j];
                 const double cA = 2.0 * t.x * f.r, cB = t.x * t.x + f.r * f.r + zl * zl;
                 double part = 0.0;
-                for (int k = 0; k < n; ++k)
-                {
-                    const double2 q = pt[k];
-                    part += q.y * q.x * rsqrt64(cB - cA * q.x);
-                }
+                if (inRange64(cB - fabs(cA), cB + fabs(cA)))
+                    for (int k = 0; k < n; ++k)
+                    {
+                        const double2 q = pt[k];
+                        part += q.y * q.x * rsqrt64u(cB - cA * q.x);
+                    }
+                else
+                    for (int k = 0; k < n; ++k)
+                    {
+                        const double2 q = pt[k];
+                        part += q.y * q.x * rsqrt64(cB - cA * q.x);
+                    }
                 sum += l.y * t.y * t.x * part;
             }
         }
@@ -111,6 +120,20 @@ __device__ __forceinline__ double segmentA64Fast(const SegmentHeader &h, const d
 // the reference's node values with every 1/sqrt(D) from rsqrt64 (fast method:
 // w c (g2 - g1) and w (p^2 - p r c) / rho^2 (top g1 - bot g2); slow method:
 // w g^3 (p^2 - p r c) and w g^3 p zl c)
+template <bool CHECKED>
+__device__ __forceinline__ void phiLoopB64(const double2 *pt, int n, double cA, double cB, double cC, double d1,
+                                           double d2, double top, double bot, double &h0, double &z0)
+{
+    for (int k = 0; k < n; ++k)
+    {
+        const double2 q = pt[k];
+        const double F = 2.0 * cB * q.x;
+        const double g1 = rsqrt64t<CHECKED>(d1 - F), g2 = rsqrt64t<CHECKED>(d2 - F);
+        h0 += q.y * q.x * (g2 - g1);
+        z0 += q.y * div64t<CHECKED>(cA - 0.5 * F, cC - F) * (top * g1 - bot * g2);
+    }
+}
+
 __device__ __forceinline__ void segmentB64Fast(const SegmentHeader &h, const double2 *tt, const double2 *lt,
                                                  const double2 *pt, const Frame &f, double &H, double &Z)
 {
@@ -125,14 +148,12 @@ __device__ __forceinline__ void segmentB64Fast(const SegmentHeader &h, const dou
             const double cA = t.x * t.x, cB = t.x * f.r, cC = cA + f.r * f.r;
             const double d1 = top * top + cC, d2 = bot * bot + cC;
             double h0 = 0.0, z0 = 0.0;
-            for (int k = 0; k < h.n_phi; ++k)
-            {
-                const double2 q = pt[k];
-                const double F = 2.0 * cB * q.x;
-                const double g1 = rsqrt64(d1 - F), g2 = rsqrt64(d2 - F);
-                h0 += q.y * q.x * (g2 - g1);
-                z0 += q.y * ((cA - 0.5 * F) / (cC - F)) * (top * g1 - bot * g2);
-            }
+            // F = 2 cB c in [-2 cB, 2 cB]: the roots' arguments d - F and the
+            // divisor cC - F (<= both) lie in [cC - 2 cB, max(d1, d2) + 2 cB]
+            if (inRange64(cC - 2.0 * fabs(cB), fmax(d1, d2) + 2.0 * fabs(cB)))
+                phiLoopB64<false>(pt, h.n_phi, cA, cB, cC, d1, d2, top, bot, h0, z0);
+            else
+                phiLoopB64<true>(pt, h.n_phi, cA, cB, cC, d1, d2, top, bot, h0, z0);
             H += t.y * t.x * h0;
             Z += t.y * z0;
         }
@@ -149,14 +170,17 @@ __device__ __forceinline__ void segmentB64Fast(const SegmentHeader &h, const dou
                 const double cA = t.x * t.x, cB = t.x * zl, cC = t.x * f.r;
                 const double cD = cA + f.r * f.r + zl * zl;
                 double h0 = 0.0, z0 = 0.0;
-                for (int k = 0; k < h.n_phi; ++k)
-                {
-                    const double2 q = pt[k];
-                    const double g = rsqrt64(cD - 2.0 * cC * q.x);
+                auto node = [&](const double2 q, double g) {
                     const double wg3 = q.y * (g * g * g);
                     z0 += wg3 * (cA - cC * q.x);
                     h0 += wg3 * (cB * q.x);
-                }
+                };
+                if (inRange64(cD - 2.0 * fabs(cC), cD + 2.0 * fabs(cC)))
+                    for (int k = 0; k < h.n_phi; ++k)
+                        node(pt[k], rsqrt64u(cD - 2.0 * cC * pt[k].x));
+                else
+                    for (int k = 0; k < h.n_phi; ++k)
+                        node(pt[k], rsqrt64(cD - 2.0 * cC * pt[k].x));
                 const double w = l.y * t.y;
                 H += w * h0;
                 Z += w * z0;

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include "fp64ops.cuh"
 #include "log64.cuh"
 
 namespace ccoil
@@ -133,6 +134,19 @@ __global__ void log64Kernel(const double *__restrict__ x, double *__restrict__ o
         out[i] = log64(x[i]);
 }
 
+__global__ void rsqrt64Kernel(const double *__restrict__ x, double *__restrict__ out, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = rsqrt64u(x[i]);
+}
+
+__global__ void div64Kernel(const double *__restrict__ num, const double *__restrict__ den, double *__restrict__ out,
+                            long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = div64u(num[i], den[i]);
+}
+
 template <typename Launch>
 float timeIt(Launch launch)
 {
@@ -232,9 +246,12 @@ extern "C" int ccoil_measure_pipe_peaks(double *fp64_tflops, double *fp32_tflops
     return CCOIL_OK;
 }
 
-extern "C" int ccoil_eval_log64(const double *x, double *out, long long n, void *stream)
+// grid-stride launch of an element-wise evaluation kernel over n elements,
+// synchronous on the stream
+template <typename Launch>
+int evalElementwise(long long n, bool pointersOk, void *stream, Launch launch)
 {
-    if (n < 0 || (n > 0 && (!x || !out)))
+    if (n < 0 || (n > 0 && !pointersOk))
         return fail(CCOIL_ERR_INVALID_ARGUMENT, "null input or output, or n < 0");
     if (n == 0)
         return CCOIL_OK;
@@ -245,9 +262,28 @@ extern "C" int ccoil_eval_log64(const double *x, double *out, long long n, void 
     if (e != cudaSuccess)
         return fail(CCOIL_ERR_NO_DEVICE, cudaGetErrorString(e));
     const long long want = (n + 255) / 256, cap = 8LL * sms;
-    log64Kernel<<<(unsigned)(want < cap ? want : cap), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, out, n);
+    launch((unsigned)(want < cap ? want : cap), static_cast<cudaStream_t>(stream));
     e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? CCOIL_OK : fail(CCOIL_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" int ccoil_eval_log64(const double *x, double *out, long long n, void *stream)
+{
+    return evalElementwise(n, x && out, stream,
+                           [&](unsigned grid, cudaStream_t st) { log64Kernel<<<grid, 256, 0, st>>>(x, out, n); });
+}
+
+extern "C" int ccoil_eval_rsqrt64(const double *x, double *out, long long n, void *stream)
+{
+    return evalElementwise(n, x && out, stream,
+                           [&](unsigned grid, cudaStream_t st) { rsqrt64Kernel<<<grid, 256, 0, st>>>(x, out, n); });
+}
+
+extern "C" int ccoil_eval_div64(const double *num, const double *den, double *out, long long n, void *stream)
+{
+    return evalElementwise(n, num && den && out, stream, [&](unsigned grid, cudaStream_t st) {
+        div64Kernel<<<grid, 256, 0, st>>>(num, den, out, n);
+    });
 }

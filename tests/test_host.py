@@ -132,10 +132,15 @@ def test_invalid_arguments_are_rejected_before_any_device_work(ccoil):
     assert L.ccoil_legendre(0, None, None) == 1
     with pytest.raises(ccoil.CCoilError):
         ccoil.legendre(101)
-    # the logarithm diagnostic: negative count, null buffers; an empty call is a no-op
+    # the FP64 diagnostics (logarithm, reciprocal square root, division): negative
+    # count, null buffers; an empty call is a no-op
     assert L.ccoil_eval_log64(None, None, -1, None) == 1
     assert L.ccoil_eval_log64(None, None, 4, None) == 1
     assert L.ccoil_eval_log64(None, None, 0, None) == 0
+    assert L.ccoil_eval_rsqrt64(None, None, 4, None) == 1
+    assert L.ccoil_eval_rsqrt64(None, None, 0, None) == 0
+    assert L.ccoil_eval_div64(None, None, None, -1, None) == 1
+    assert L.ccoil_eval_div64(None, None, None, 0, None) == 0
 
 
 def test_cpu_compute_methods_are_not_provided(ccoil):
