@@ -103,8 +103,7 @@ def lib():
                                           ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int, vp]
     L.ccoil_self_inductances.argtypes = [cp, pp, ctypes.c_int, vp, vp]
     L.ccoil_eval_log64.argtypes = [vp, vp, ctypes.c_longlong, vp]
-    L.ccoil_eval_rsqrt64.argtypes = [vp, vp, ctypes.c_longlong, vp]
-    L.ccoil_eval_div64.argtypes = [vp, vp, vp, ctypes.c_longlong, vp]
+    L.ccoil_eval_fp64_op.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_longlong, vp]
     L.ccoil_pair_arrangements_zaxis.argtypes = [cp, ctypes.c_int, cp, pp, pp, vp, vp, ctypes.c_longlong,
                                                 ctypes.c_int, ctypes.c_int, vp, ctypes.POINTER(ctypes.c_longlong),
                                                 ctypes.c_int, vp]

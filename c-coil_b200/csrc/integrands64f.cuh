@@ -29,6 +29,13 @@
 // Against 40-digit arithmetic a pair is within 1.1e-11 (relative) where the
 // reference's sequence is off by up to 2e-10.
 // Slow method: w c p / sqrt(D) per node, as the reference.
+// log(n / d): logRatio64 on the unchecked path, log64 of the IEEE quotient on
+// the checked one
+template <bool CHECKED> __device__ __forceinline__ double logRatio64t(double n, double d)
+{
+    return CHECKED ? log64(n / d) : logRatio64(n, d);
+}
+
 // One thickness node of the fast method: sum over the angular nodes.
 template <bool PAIRED, bool CHECKED>
 __device__ __forceinline__ double phiLoopA64(const double2 *pt, int n, double cA, double cB, double T2, double B2,
@@ -47,7 +54,7 @@ __device__ __forceinline__ double phiLoopA64(const double2 *pt, int n, double cA
         double n1, e1, n2, e2;
         ratio(q.x, n1, e1);
         ratio(qm.x, n2, e2);
-        part += 0.5 * (q.y * q.x - qm.y * qm.x) * log64(div64t<CHECKED>(n1 * e2, e1 * n2));
+        part += 0.5 * (q.y * q.x - qm.y * qm.x) * logRatio64t<CHECKED>(n1 * e2, e1 * n2);
     }
     if (n & 1)
     {
@@ -55,7 +62,7 @@ __device__ __forceinline__ double phiLoopA64(const double2 *pt, int n, double cA
         const double2 q = pt[PAIRED ? n - 1 : n / 2];
         double n1, e1;
         ratio(q.x, n1, e1);
-        part += q.y * q.x * log64(div64t<CHECKED>(n1, e1));
+        part += q.y * q.x * logRatio64t<CHECKED>(n1, e1);
     }
     return part;
 }

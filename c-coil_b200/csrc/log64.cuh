@@ -64,4 +64,45 @@ __device__ __forceinline__ double log64(double x)
     return sum + (err + small);
 }
 
+// log(n / d) for positive normal n and d: n is brought to d's binary exponent
+// (n' = n 2^-k, exact) and, by one factor of 2, to n' / d in [sqrt(1/2),
+// sqrt(2)); then log(n / d) = k ln 2 + 2 atanh(f), f = (n' - d) / (n' + d), by
+// the series above.  n' - d is exact (Sterbenz: n' and d within a factor 2), so
+// f keeps its relative accuracy however close n / d is to 1, which a rounded
+// quotient n / d would not; the quotient takes one Newton-Raphson step on the
+// reciprocal estimate and a residual correction, and the low parts log64
+// carries are dropped: within a few ulp of log(n / d).  Used by the FP64
+// refinement forms of the vector potential (a ratio of products of distances).
+__device__ __forceinline__ double logRatio64(double n, double d)
+{
+    constexpr double kLn2 = 0.6931471805599453;
+    constexpr double kSqrt2 = 1.4142135623730951, kSqrtHalf = 0.7071067811865476;
+    const long long bn = __double_as_longlong(n), bd = __double_as_longlong(d);
+    long long k = (bn >> 52) - (bd >> 52);
+    double m = __longlong_as_double(bn - (k << 52));
+    const bool up = m >= kSqrt2 * d, down = m < kSqrtHalf * d;
+    m = up ? 0.5 * m : (down ? 2.0 * m : m);
+    k += (long long)up - (long long)down;
+    const double g = m - d;  // exact
+    const double t = m + d;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(t));
+    y = fma(y, fma(-t, y, 1.0), y);
+    const double q = g * y;
+    const double f = fma(fma(-q, t, g), y, q);
+    const double z = f * f;
+    double p = 1.0 / 21.0;
+    p = fma(p, z, 1.0 / 19.0);
+    p = fma(p, z, 1.0 / 17.0);
+    p = fma(p, z, 1.0 / 15.0);
+    p = fma(p, z, 1.0 / 13.0);
+    p = fma(p, z, 1.0 / 11.0);
+    p = fma(p, z, 1.0 / 9.0);
+    p = fma(p, z, 1.0 / 7.0);
+    p = fma(p, z, 1.0 / 5.0);
+    p = fma(p, z, 1.0 / 3.0);
+    const double f2 = 2.0 * f;
+    return fma((double)k, kLn2, fma(f2 * z, p, f2));
+}
+
 #endif

@@ -134,17 +134,13 @@ __global__ void log64Kernel(const double *__restrict__ x, double *__restrict__ o
         out[i] = log64(x[i]);
 }
 
-__global__ void rsqrt64Kernel(const double *__restrict__ x, double *__restrict__ out, long long n)
+// op 0: 1/sqrt(a), 1: sqrt(a), 2: a / b, 3: log(a / b), by the FP64 forms of
+// the refinement pass
+__global__ void fp64OpKernel(int op, const double *__restrict__ a, const double *__restrict__ b,
+                             double *__restrict__ out, long long n)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        out[i] = rsqrt64u(x[i]);
-}
-
-__global__ void div64Kernel(const double *__restrict__ num, const double *__restrict__ den, double *__restrict__ out,
-                            long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        out[i] = div64u(num[i], den[i]);
+        out[i] = op == 0 ? rsqrt64u(a[i]) : op == 1 ? sqrt64u(a[i]) : op == 2 ? div64u(a[i], b[i]) : logRatio64(a[i], b[i]);
 }
 
 template <typename Launch>
@@ -275,15 +271,11 @@ extern "C" int ccoil_eval_log64(const double *x, double *out, long long n, void 
                            [&](unsigned grid, cudaStream_t st) { log64Kernel<<<grid, 256, 0, st>>>(x, out, n); });
 }
 
-extern "C" int ccoil_eval_rsqrt64(const double *x, double *out, long long n, void *stream)
+extern "C" int ccoil_eval_fp64_op(int op, const double *a, const double *b, double *out, long long n, void *stream)
 {
-    return evalElementwise(n, x && out, stream,
-                           [&](unsigned grid, cudaStream_t st) { rsqrt64Kernel<<<grid, 256, 0, st>>>(x, out, n); });
-}
-
-extern "C" int ccoil_eval_div64(const double *num, const double *den, double *out, long long n, void *stream)
-{
-    return evalElementwise(n, num && den && out, stream, [&](unsigned grid, cudaStream_t st) {
-        div64Kernel<<<grid, 256, 0, st>>>(num, den, out, n);
+    if (op < 0 || op > 3)
+        return fail(CCOIL_ERR_INVALID_ARGUMENT, "op must be 0 (rsqrt), 1 (sqrt), 2 (divide) or 3 (log of a ratio)");
+    return evalElementwise(n, a && out && (op < 2 || b), stream, [&](unsigned grid, cudaStream_t st) {
+        fp64OpKernel<<<grid, 256, 0, st>>>(op, a, b, out, n);
     });
 }

@@ -414,15 +414,15 @@ int ccoil_measure_op_rates(double *rates, int count);
  * every x must be positive, normal and finite.  Synchronous on `stream`. */
 int ccoil_eval_log64(const double *x, double *out, long long n, void *stream);
 
-/* Diagnostics with no counterpart in the reference: the reciprocal square root
- * and the division that the FP32_REFINED refinement pass and the FP64 nodes of
- * the FP32 arrangement kernels use (FP64 estimates refined by Newton-Raphson
- * steps, within about 1 ulp), at n points, for checks against other
- * implementations: out[i] = 1 / sqrt(x[i]) and out[i] = num[i] / den[i].  All
- * pointers are device pointers of n doubles; every x and den must lie in
- * [1e-36, 1e36] and every num must be finite.  Synchronous on `stream`. */
-int ccoil_eval_rsqrt64(const double *x, double *out, long long n, void *stream);
-int ccoil_eval_div64(const double *num, const double *den, double *out, long long n, void *stream);
+/* Diagnostic with no counterpart in the reference: the FP64 forms that the
+ * FP32_REFINED refinement pass and the FP64 nodes of the FP32 arrangement
+ * kernels use (FP64 estimates refined by Newton-Raphson steps), at n points,
+ * for checks against other implementations.  op 0: out[i] = 1 / sqrt(a[i]);
+ * 1: sqrt(a[i]); 2: a[i] / b[i]; 3: log(a[i] / b[i]) (b unused and may be NULL
+ * for ops 0 and 1).  All pointers are device pointers of n doubles; a (ops 0,
+ * 1) and b (op 2) must lie in [1e-36, 1e36], a in op 2 be finite, a and b in
+ * op 3 be positive, normal and finite.  Synchronous on `stream`. */
+int ccoil_eval_fp64_op(int op, const double *a, const double *b, double *out, long long n, void *stream);
 
 #ifdef __cplusplus
 }

@@ -137,10 +137,10 @@ def test_invalid_arguments_are_rejected_before_any_device_work(ccoil):
     assert L.ccoil_eval_log64(None, None, -1, None) == 1
     assert L.ccoil_eval_log64(None, None, 4, None) == 1
     assert L.ccoil_eval_log64(None, None, 0, None) == 0
-    assert L.ccoil_eval_rsqrt64(None, None, 4, None) == 1
-    assert L.ccoil_eval_rsqrt64(None, None, 0, None) == 0
-    assert L.ccoil_eval_div64(None, None, None, -1, None) == 1
-    assert L.ccoil_eval_div64(None, None, None, 0, None) == 0
+    assert L.ccoil_eval_fp64_op(0, None, None, None, 4, None) == 1
+    assert L.ccoil_eval_fp64_op(2, None, None, None, -1, None) == 1
+    assert L.ccoil_eval_fp64_op(4, None, None, None, 0, None) == 1
+    assert L.ccoil_eval_fp64_op(3, None, None, None, 0, None) == 0
 
 
 def test_cpu_compute_methods_are_not_provided(ccoil):
