@@ -422,6 +422,13 @@ __device__ __forceinline__ void transformDerivatives(double yA, double zA, doubl
 #ifndef CCOIL_PAIR32_MIN_BLOCKS
 #define CCOIL_PAIR32_MIN_BLOCKS 9
 #endif
+// the FP32_REFINED variants, whose refined nodes run the FP64 forms: 9 measured
+// as fast as 8, 7 and 6 (80 registers) at the fractions that reach 1e-7 (M
+// 124.4 against 124.7-126.5 ms at 2^18 arrangements; F/T 104.1 against
+// 103.0-104.1 ms), and faster at the default fraction (M 72.1 against 73.9-76.0)
+#ifndef CCOIL_PAIR32R_MIN_BLOCKS
+#define CCOIL_PAIR32R_MIN_BLOCKS 9
+#endif
 // FP32_REFINED arrangements: the largest scratch of node contributions (the
 // grid shrinks to fit it)
 constexpr size_t kPairRefineScratchBytes = size_t(1) << 30;
@@ -533,7 +540,8 @@ __device__ __noinline__ double2 pairB32(const SegmentHeader &h, const double2 *t
 // that dominate an arrangement whose ring sum cancels, whose FP32 errors the
 // cancellation magnifies.
 template <int QTY, bool FP32, bool REFINE = false>
-__global__ void __launch_bounds__(128, FP32 ? CCOIL_PAIR32_MIN_BLOCKS : CCOIL_PAIR_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, FP32 ? (REFINE ? CCOIL_PAIR32R_MIN_BLOCKS : CCOIL_PAIR32_MIN_BLOCKS)
+                                               : CCOIL_PAIR_MIN_BLOCKS)
     pairKernel64(const unsigned char *__restrict__ blob, const long long *__restrict__ primOffsets, int nprim,
                  const double *__restrict__ primPoses, const double *__restrict__ secPoses, long long count,
                  double *__restrict__ out, unsigned long long *__restrict__ zAxisCount, int stagedBytes,
