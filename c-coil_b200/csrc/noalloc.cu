@@ -135,6 +135,14 @@ extern "C" int ccoil_fields_fp32c_static(const ccoil_coil_t *coils, int coil_cou
     const int width = field == CCOIL_FIELD_G ? 9 : 3;
     if (point_count == 0)
         return CCOIL_OK;
+    // a captured call would record copies from the shared host staging buffers,
+    // which a replay reads after later calls have overwritten them
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    const cudaError_t ce = cudaStreamIsCapturing(st, &capture);
+    if (ce != cudaSuccess)
+        return failMessage(CCOIL_ERR_CUDA, cudaGetErrorString(ce));
+    if (capture != cudaStreamCaptureStatusNone)
+        return failMessage(CCOIL_ERR_NOT_SUPPORTED, "not supported during stream capture");
 
     unsigned char *scratch = nullptr;
     int rc = scratchAddress(&scratch);

@@ -382,9 +382,11 @@ int ccoil_inject_allocation_failures(int count);
  * 3 MiB array in device memory, held by every GPU that loads the library until
  * the process exits.  Limits: at most 1 MiB of node tables (about 400 coils at
  * PrecisionFactor 5), 8192 segments and 2^31-1 points; larger requests return
- * CCOIL_ERR_INVALID_ARGUMENT with a message.  The first call on a device looks
- * up the array's device address; make that first call before any stream
- * capture.  The address is kept for the life of the process, so
+ * CCOIL_ERR_INVALID_ARGUMENT with a message.  A call on a stream that is being
+ * captured returns CCOIL_ERR_NOT_SUPPORTED: every call stages the node tables
+ * through one shared host buffer, which a graph replay would read after later
+ * calls had overwritten it.  The first call on a device looks up the array's
+ * device address and keeps it for the life of the process, so
  * cudaDeviceReset is not supported while the library is in use.  All calls
  * share the array: calls that overlap on the GPU (other streams or host
  * threads) race and must be ordered by the caller. */

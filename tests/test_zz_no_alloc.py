@@ -63,3 +63,37 @@ def test_static_entry_point_rejects_oversized_requests(ccoil):
     rc = fn(structs, 1200, ctypes.c_void_p(pts.data_ptr()), 4, 1, ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 1
     assert b"1 MiB" in L.ccoil_last_error_message()
+
+
+def test_static_entry_point_refuses_stream_capture(ccoil):
+    """Inside a stream capture the entry point returns CCOIL_ERR_NOT_SUPPORTED
+    before it touches the stream (a captured call would record copies from the
+    shared host staging buffers), and the capture itself stays usable."""
+    import torch
+    from ccoil_b200 import workloads
+
+    L = ccoil.lib()
+    fn = L.ccoil_fields_fp32c_static
+    fn.argtypes = [ctypes.POINTER(ccoil._lib.CoilStruct), ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                   ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    coils = workloads.coils_from_rows(workloads.coil_rows_mixed(4, seed=317), 5.0)
+    structs = (ccoil._lib.CoilStruct * len(coils))(*[c.struct() for c in coils])
+    dpts = torch.from_numpy(workloads.points_cube(256, seed=318)).cuda()
+    dout = torch.empty((256, 3), dtype=torch.float64, device="cuda")
+    x = torch.zeros(1, device="cuda")
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        x.add_(1.0)
+        rc = fn(structs, len(coils), ctypes.c_void_p(dpts.data_ptr()), 256, 1, ctypes.c_void_p(dout.data_ptr()),
+                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 4, rc  # CCOIL_ERR_NOT_SUPPORTED
+    assert b"capture" in L.ccoil_last_error_message()
+    g.replay()
+    torch.cuda.synchronize()
+    assert x.item() == 1.0
+    # outside a capture the same call runs
+    assert fn(structs, len(coils), ctypes.c_void_p(dpts.data_ptr()), 256, 1, ctypes.c_void_p(dout.data_ptr()),
+              None) == 0
+    torch.cuda.synchronize()
+    assert torch.isfinite(dout).all()
