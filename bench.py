@@ -208,26 +208,36 @@ def bench_arrangements(a, cc, workloads, dev, rank, max_over_ranks, barrier, mod
                 res[key + "_errors"] = {"M": rel_err_stats(m32, m64), "F": rel_err_stats(f32[:, :3], f64[:, :3]),
                                         "T": rel_err_stats(f32[:, 3:], f64[:, 3:])}
         if "fp32r" in res:
-            # the arrangements at max error <= 1e-7: FP32_REFINED at the fractions that
-            # reach it on this workload (M 0.01, F/T 0.005), checked here against FP64;
-            # FP64 itself where the check fails
+            # the arrangements at max error <= 1e-7: FP32_REFINED at the fraction that
+            # reaches it on this workload (M 0.01, F/T 0.005) and at fraction 0 (every
+            # node in the FP64 refinement forms, no FP32 pass), each checked here
+            # against FP64; the faster passing one is reported (FP64 where none passes)
             import ctypes
             L = cc.lib()
             default = L.ccoil_refine_fraction()
             at = {}
             try:
-                for name, q, w, fr in (("M", 0, 1, 0.01), ("FT", 1, 6, 0.005)):
-                    L.ccoil_set_refine_fraction(ctypes.c_double(fr))
-                    r = timed(q, w, cc.PrecisionMode.FP32_REFINED)
+                for name, q, w, fractions in (("M", 0, 1, (0.01, 0.0)), ("FT", 1, 6, (0.005, 0.0))):
                     ref = res["fp64"][name]["out"]
-                    errs = ({"M": rel_err_stats(r["out"], ref)} if name == "M" else
-                            {"F": rel_err_stats(r["out"][:, :3], ref[:, :3]),
-                             "T": rel_err_stats(r["out"][:, 3:], ref[:, 3:])})
-                    ok = all(e["max"] <= 1e-7 for e in errs.values())
-                    src = r if ok else res["fp64"][name]
-                    at[name] = {"precision_mode": ("FP32_REFINED, fraction %g" % fr) if ok else "FP64",
-                                "arrangements_per_s": src["arrangements_per_s"], "ms": src["ms"],
-                                "refined_max_error": {k: e["max"] for k, e in errs.items()}}
+                    cands = {}
+                    for fr in fractions:
+                        L.ccoil_set_refine_fraction(ctypes.c_double(fr))
+                        r = timed(q, w, cc.PrecisionMode.FP32_REFINED)
+                        errs = ({"M": rel_err_stats(r["out"], ref)} if name == "M" else
+                                {"F": rel_err_stats(r["out"][:, :3], ref[:, :3]),
+                                 "T": rel_err_stats(r["out"][:, 3:], ref[:, 3:])})
+                        cands["%g" % fr] = {"ms": r["ms"], "arrangements_per_s": r["arrangements_per_s"],
+                                            "max_error": {k: e["max"] for k, e in errs.items()},
+                                            "passes": all(e["max"] <= 1e-7 for e in errs.values())}
+                    passing = [f for f, c in cands.items() if c["passes"]]
+                    if passing:
+                        best = min(passing, key=lambda f: cands[f]["ms"])
+                        src = cands[best]
+                        mode = "FP32_REFINED, fraction %s" % best + (" (every node in FP64)" if float(best) == 0 else "")
+                    else:
+                        src, mode = res["fp64"][name], "FP64"
+                    at[name] = {"precision_mode": mode, "arrangements_per_s": src["arrangements_per_s"],
+                                "ms": src["ms"], "refined_max_error": src.get("max_error"), "candidates": cands}
             finally:
                 L.ccoil_set_refine_fraction(ctypes.c_double(default))
             res["at_1e-7"] = at
@@ -550,7 +560,7 @@ def refine_sweep_arrangements(a, cc, workloads, dev, L, default_fraction):
     _, _, pstruct, sstruct, spre, pposes, sposes, _ = pair_setup(cc, workloads, a.arrangements, 3)
     dp = torch.from_numpy(pposes).to(dev)
     ds = torch.from_numpy(sposes).to(dev)
-    fractions = [0.1, 0.03, 0.01, 0.005, 0.003]
+    fractions = [0.1, 0.03, 0.01, 0.005, 0.003, 0.0]  # 0: every node in FP64, no FP32 pass
 
     def timed(q, w, mode):
         out = torch.empty((a.arrangements, w), dtype=torch.float64, device=dev)
@@ -855,7 +865,8 @@ def main():
                 roof[q] = {"achieved": 2.0 * slots / t / 1e12, "peak": 2.0 * rates[0] / 1e12, "unit": "TFLOP/s",
                            "frac": slots / t / rates[0]}
             line["arrangements"]["fp64_roofline"] = roof
-        line["gpu_launches"] += 2 * a.steps * (len(modes) + (1 if "at_1e-7" in arr else 0))
+        # timed launches: M and F/T per precision mode, and per candidate of the 1e-7 configuration
+        line["gpu_launches"] += 2 * a.steps * (len(modes) + (2 if "at_1e-7" in arr else 0))
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, cores, dt, desc = cpu_reference_rate(a, a.cpu_sample_points)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",

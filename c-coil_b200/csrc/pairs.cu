@@ -883,9 +883,15 @@ __global__ void __launch_bounds__(128, FP32 ? (REFINE ? CCOIL_PAIR32R_MIN_BLOCKS
                 __syncwarp();
                 nNear = rest;
             };
+            // REFINE at fraction 0 refines every node: each node in the FP64 forms
+            // directly, without the FP32 pass
+            const bool allFp64 = REFINE && !(fraction > 0.0);
             if (!FP32)
                 for (int n0 = 0; n0 < nsec; n0 += 32)
                     node(n0 + lane < nsec ? n0 + lane : nsec - 1, n0 + lane < nsec, 0);
+            else if (allFp64)
+                for (int n0 = 0; n0 < nsec; n0 += 32)
+                    node(n0 + lane < nsec ? n0 + lane : nsec - 1, n0 + lane < nsec, 2);
             else
                 for (int n0 = 0; n0 < nsec || nNear > 0;)
                 {
@@ -897,7 +903,7 @@ __global__ void __launch_bounds__(128, FP32 ? (REFINE ? CCOIL_PAIR32R_MIN_BLOCKS
                         n0 += 32;
                     }
                 }
-            if (REFINE)
+            if (REFINE && !allFp64)
             {
                 // the primary's totals (every lane), then the dominating nodes in FP64;
                 // node n was evaluated, and its contribution stored, by lane n % 32

@@ -268,7 +268,10 @@ typedef struct ccoil_pose
  * CCOIL_PRECISION_FP32_REFINED (mutual inductance and force/torque) also
  * re-evaluates in FP64 every secondary node whose contribution exceeds the
  * refinement fraction of the arrangement's M (of its force or of its torque);
- * it keeps each warp's node contributions in up to 1 GiB of device scratch. */
+ * it keeps each warp's node contributions in up to 1 GiB of device scratch.
+ * At fraction 0 every node is refined, so the FP32 pass is skipped: each node
+ * is evaluated once in those FP64 forms (within about 1e-11 of
+ * CCOIL_PRECISION_FP64, in about half its time). */
 int ccoil_pair_arrangements(const ccoil_coil_t *primaries, int primary_count, const ccoil_coil_t *secondary,
                             const ccoil_precision_args_t *secondary_precisions, const ccoil_pose_t *primary_poses,
                             const ccoil_pose_t *secondary_poses, long long count, int quantity, int precision,
